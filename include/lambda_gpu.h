@@ -1,0 +1,270 @@
+/*
+ * lambda_gpu.h — C ABI of the B200 (sm_100a) spectral path-tracing library.
+ *
+ * This is the drop-in boundary for lambda's render call.  The reference
+ * renders with the C++ member call
+ *
+ *     void Renderer::render(nl::cg::scene const&, rendering&);
+ *         declared  include/renderer.hpp:39, defined src/renderer.cpp:14,
+ *         called    src/main.cpp:41
+ *
+ * and has no plugin or FFI layer.  A host that keeps the reference's .nls
+ * loader, scene structures and CLI flattens its nl::cg::scene into the plain
+ * structs below (pointers into the host's own vectors; nothing is copied on
+ * the host), calls lgpu_upload_scene + lgpu_render, and receives the linear
+ * BT.709 image in the reference's layout (row 0 at the top, W*H*3 floats,
+ * normalised by 1/(SPP*HERO_SAMPLES), src/renderer.cpp:52-56).
+ *
+ * Conventions for every entry point:
+ *   - returns LGPU_OK (0) or a negative lgpu_status; the message of the last
+ *     failure is available from lgpu_last_error(ctx);
+ *   - no C++ exception crosses the boundary;
+ *   - calls are synchronous unless the name ends in _async;
+ *   - one context per host thread; device memory is owned by the context;
+ *   - no torch types: plain pointers and sizes only.
+ */
+#ifndef LAMBDA_GPU_H
+#define LAMBDA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LGPU_ABI_VERSION 1
+
+typedef struct lgpu_ctx lgpu_ctx;
+
+typedef enum lgpu_status {
+  LGPU_OK = 0,
+  LGPU_ERR_INVALID_ARGUMENT = -1,
+  LGPU_ERR_CUDA = -2,
+  LGPU_ERR_OUT_OF_MEMORY = -3,
+  LGPU_ERR_NO_SCENE = -4,
+  LGPU_ERR_UNSUPPORTED = -5,
+  /* a device-side check fired (traversal stack overflow, index out of
+     range); the kernel skipped the offending access and reported it */
+  LGPU_ERR_DEVICE_CHECK = -6,
+  /* a bounded device-side wait ran out before its condition held */
+  LGPU_ERR_TIMEOUT = -7,
+  LGPU_ERR_NO_DEVICE = -8
+} lgpu_status;
+
+/* ---- scene description ------------------------------------------------ */
+
+/* Variant order of nl::cg::Object (cg.hpp:857). */
+typedef enum lgpu_object_type {
+  LGPU_OBJ_SPHERE = 0,
+  LGPU_OBJ_PLANE = 1,
+  LGPU_OBJ_TRIMESH = 2
+} lgpu_object_type;
+
+/* Variant order of nl::cg::Material (cg.hpp:1084-1085). */
+typedef enum lgpu_material_type {
+  LGPU_MAT_LAMBERTIAN = 0,
+  LGPU_MAT_BLINN = 1,
+  LGPU_MAT_THINFILM = 2,
+  LGPU_MAT_MICROFACET = 3, /* loaded by the reference but never shaded */
+  LGPU_MAT_EMITTER = 4,
+  LGPU_MAT_DIREMITTER = 5
+} lgpu_material_type;
+
+/* Variant order of nl::cg::Light (cg.hpp:904-905). */
+typedef enum lgpu_light_type {
+  LGPU_LIGHT_AMBIENT = 0,
+  LGPU_LIGHT_POINT = 1,
+  LGPU_LIGHT_DIR = 2,
+  LGPU_LIGHT_SPHERE = 3,
+  LGPU_LIGHT_QUADDIR = 4
+} lgpu_light_type;
+
+/* nl::cg::transform (cg.hpp:422-425): row-major 4x4 M and its inverse. */
+typedef struct lgpu_transform {
+  float M[16];
+  float M_inv[16];
+} lgpu_transform;
+
+/* nl::cg::camera (cg.hpp:1151-1165) after camera::init. */
+typedef struct lgpu_camera {
+  float base_x[3], base_y[3], base_z[3]; /* camera::base */
+  float pos[3];
+  float fov, dof, D, delta, h, w; /* delta = camera::Δ */
+  uint64_t width, height;
+} lgpu_camera;
+
+/* Spectral discretisation.  The reference compiles it in: Nλ = 80 bins on
+   [400, 720] nm and HERO_SAMPLES = 16 (cg.hpp:40-41, 244-245).  The CMF
+   tables are the host's coefficientλ<Nλ> CMF_X/Y/Z (cg.hpp:329-331). */
+typedef struct lgpu_spectral {
+  uint32_t n_bins;
+  uint32_t hero_k; /* 4, 8 or 16 */
+  float lambda_inf, lambda_sup;
+  const float* cmf_x; /* n_bins each */
+  const float* cmf_y;
+  const float* cmf_z;
+} lgpu_spectral;
+
+/* One entry of nl::cg::list<Material>.  Spectra are indices into
+   lgpu_scene::spectra (-1 when unused):
+     lambertian : s[0] = albedo                         (cg.hpp:921-926)
+     blinn      : s[0..4] = Kd, Ks, Kt, Le, ior          (cg.hpp:927-993)
+     thinfilm   : s[0] = film_ior, s[1] = base_ior       (cg.hpp:995-1052)
+     emitter    : s[0] = radiance                        (cg.hpp:1069-1074)
+     diremitter : s[0] = radiance, specular              (cg.hpp:1075-1081)
+   Blinn's p_d, p_spec, w_r, w_t are the values blinn::init computed. */
+typedef struct lgpu_material {
+  int32_t type;
+  int32_t spectrum[5];
+  float alpha;
+  float p_d, p_spec, w_r, w_t;
+  float d;
+  float specular;
+} lgpu_material;
+
+/* One entry of nl::cg::list<Object> (cg.hpp:835-857); the object index is
+   its position in the array (the reference's objectidx). */
+typedef struct lgpu_object {
+  int32_t type;
+  uint32_t mat;
+  uint32_t mesh; /* trimesh only */
+  uint32_t reserved;
+  lgpu_transform T;
+} lgpu_object;
+
+/* One entry of nl::cg::list<Light> (cg.hpp:875-905). */
+typedef struct lgpu_light {
+  int32_t type;
+  int32_t spectrum; /* radiance or radiant_intensity */
+  uint32_t obj;     /* sphere / quaddir: the light's own object index */
+  float size;       /* spherelight::size */
+  float inv_area;   /* quaddirlight::inv_area */
+  float spec;       /* quaddirlight::spec */
+  float pos[3];     /* pointlight::pos */
+  float dir[3];     /* dirlight::dir */
+  lgpu_transform T; /* _sphere.T / _plane.T */
+} lgpu_light;
+
+/* nl::cg::trimeshdata (cg.hpp:766-820) with its wide BVH in the reference's
+   own layout (cg.hpp:596-631): nodes are {childrenbb_idx, data} pairs with
+   data = idx<<4 | (count-1)<<1 | leaf; bbs are aabb_avx2 records of 48
+   floats (inf[3][8] then sup[3][8]); prim_idxs index faces.  Position and
+   normal arrays include fast_obj's dummy element at index 0. */
+typedef struct lgpu_mesh {
+  uint32_t n_positions, n_normals, n_faces;
+  uint32_t f_stride; /* uint32 words per face in F (9 for nl::cg::triangle) */
+  const float* V;    /* n_positions * 3 */
+  const float* N;    /* n_normals * 3 */
+  const uint32_t* F; /* face f: V idx at F[f*f_stride+0..2], N idx at +3..5 */
+  const float* GN;   /* n_faces * 3 geometric normals */
+  float bounds[6];   /* trimeshdata::bounds: inf xyz, sup xyz */
+  uint32_t n_nodes, n_bbs, n_prim_idxs, reserved;
+  const uint32_t* nodes;
+  const float* bbs;
+  const uint32_t* prim_idxs;
+} lgpu_mesh;
+
+typedef struct lgpu_scene {
+  lgpu_camera cam;
+  lgpu_spectral spec;
+  uint32_t n_objects, n_materials, n_lights, n_meshes, n_spectra, reserved;
+  const lgpu_object* objects;
+  const lgpu_material* materials;
+  const lgpu_light* lights;
+  const lgpu_mesh* meshes;
+  const float* spectra; /* n_spectra * spec.n_bins */
+} lgpu_scene;
+
+/* ---- rendering -------------------------------------------------------- */
+
+/* Traverse objects in the reference's order (linear object loop, children
+   sorted far-to-near, cg.hpp:1436-1437, 1477-1487) so that equal-t ties
+   resolve exactly as the reference does.  Without it the device uses its
+   instance-level BVH. */
+#define LGPU_FLAG_REFERENCE_ORDER 0x1u
+
+/* Renderer settings (include/renderer.hpp:35-37) plus the device RNG seed. */
+typedef struct lgpu_render_params {
+  uint32_t spp;             /* Renderer::SPP */
+  uint32_t max_scatterings; /* Renderer::MAX_SCATTERINGS */
+  float sample_p;           /* Renderer::SAMPLE_P */
+  uint32_t flags;
+  uint64_t seed;
+  uint32_t spp_offset; /* index of the first sample (progressive renders) */
+  uint32_t reserved;
+} lgpu_render_params;
+
+/* Result of one closest-hit query (nl::cg::hitinfo, cg.hpp:1138-1149). */
+typedef struct lgpu_hit {
+  float t;       /* hitinfo::z; FLT_MAX on a miss */
+  uint32_t obj;  /* UINT32_MAX on a miss */
+  uint32_t face; /* trimesh face; UINT32_MAX for spheres and planes */
+  uint32_t mat;
+  float p[3];  /* world-space hit point */
+  float n[3];  /* shading frame z (hitinfo::F.z) */
+  float gn[3]; /* geometric normal */
+  uint32_t front;
+} lgpu_hit;
+
+typedef struct lgpu_stats {
+  double last_kernel_ms;  /* device time of the last render/trace kernel */
+  uint64_t rays;          /* extension + shadow rays of the last render */
+  uint64_t paths;
+  uint32_t device_checks;   /* device-side checks that fired */
+  uint32_t max_stack;       /* traversal stack bound in use */
+  uint32_t nonfinite_paths; /* paths whose radiance was NaN or infinite */
+  uint32_t reserved;
+} lgpu_stats;
+
+/* Context.  `device` is a CUDA ordinal. */
+int lgpu_create(int device, lgpu_ctx** out);
+void lgpu_destroy(lgpu_ctx* ctx);
+const char* lgpu_last_error(const lgpu_ctx* ctx);
+int lgpu_abi_version(void);
+
+/* Copies the scene to the device and lays it out for traversal (replaces
+   the implicit scene access of Renderer::render, src/renderer.cpp:14). The
+   host keeps ownership of every array it passed. */
+int lgpu_upload_scene(lgpu_ctx* ctx, const lgpu_scene* scene);
+
+/* Renderer::render (src/renderer.cpp:14-61): renders the uploaded scene into
+   the host buffer out_linrgb (cam.width*cam.height*3 floats, row 0 at the
+   top). */
+int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linrgb);
+
+/* Same as lgpu_render with the output in device memory, on `stream`
+   (a cudaStream_t, or NULL for the context's stream). */
+int lgpu_render_device(lgpu_ctx* ctx, const lgpu_render_params* params,
+                       float* d_out_linrgb, void* stream);
+
+/* intersect::scene (cg.hpp:1469-1489) on n rays given as 6 floats each
+   (origin xyz, direction xyz) in host memory; writes n lgpu_hit. */
+int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,
+                       uint32_t flags, lgpu_hit* out);
+
+/* Renderer::toneMap (src/renderer.cpp:149-176) followed by the 8-bit sRGB
+   encode of rendering::rgb24 (include/renderer.hpp:20-29).  Either output
+   may be NULL.  Host buffers of w*h*3 elements. */
+int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h,
+                 float y_mid, float* out_tonemapped, uint8_t* out_rgb24);
+
+int lgpu_get_stats(const lgpu_ctx* ctx, lgpu_stats* out);
+
+/* Host utility for hosts without the reference's builder: builds the wide
+   BVH of one mesh exactly as bvh::build does (cg.hpp:632-749), in the
+   reference's layout (see lgpu_mesh).  Every interior node has at least two
+   children, so nodes <= 2*n_faces and bbs records <= 2*n_faces: output
+   arrays of 4*n_faces words (nodes), 96*n_faces floats (bbs) and n_faces
+   words (prim_idxs) always suffice; NULL outputs only return the counts
+   (n_nodes counts nodes, n_bbs counts 48-float records). */
+int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
+                   uint32_t f_stride, uint32_t n_faces, uint32_t* nodes,
+                   uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
+                   uint32_t* prim_idxs, uint32_t* n_prim_idxs);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LAMBDA_GPU_H */

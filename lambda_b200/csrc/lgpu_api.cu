@@ -1,0 +1,364 @@
+// lgpu_api.cu — the extern "C" entry points of include/lambda_gpu.h.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "lambda_gpu.h"
+#include "lgpu_kernels.cuh"
+#include "lgpu_layout.h"
+
+using namespace lgpu;
+
+namespace {
+
+template <class T>
+struct DevArray {
+  T* ptr = nullptr;
+  size_t n = 0;
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace
+
+struct lgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  bool has_scene = false;
+  DevScene S{};
+  lgpu_stats stats{};
+  // scene arrays
+  DevArray<DevObject> objects;
+  DevArray<DevMesh> meshes;
+  DevArray<WideNode> nodes;
+  DevArray<TriSlot> tris;
+  DevArray<FaceShade> shade;
+  DevArray<float> spectra;
+  DevArray<DevMaterial> mats;
+  DevArray<lgpu_light> lights;
+  DevArray<uint32_t> tlas_objects;
+  DevArray<float> cmf;
+  // working buffers
+  DevArray<float> out;
+  DevArray<float> rays;
+  DevArray<lgpu_hit> hits;
+  DevArray<double> partials;
+  DevArray<float> tm_in, tm_out;
+  DevArray<uint8_t> tm_24;
+  DevCounters* counters = nullptr;
+  float* exposure = nullptr;
+
+  void release_scene() {
+    objects.release();
+    meshes.release();
+    nodes.release();
+    tris.release();
+    shade.release();
+    spectra.release();
+    mats.release();
+    lights.release();
+    tlas_objects.release();
+    cmf.release();
+    has_scene = false;
+  }
+};
+
+namespace {
+
+int fail(lgpu_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_fail(lgpu_ctx* ctx, cudaError_t e, const char* what) {
+  int const code = (e == cudaErrorMemoryAllocation) ? LGPU_ERR_OUT_OF_MEMORY : LGPU_ERR_CUDA;
+  return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <class T>
+cudaError_t upload(DevArray<T>& d, const std::vector<T>& h, cudaStream_t st) {
+  d.release();
+  size_t const n = h.empty() ? 1 : h.size();
+  cudaError_t e = cudaMalloc(&d.ptr, n * sizeof(T));
+  if (e != cudaSuccess) return e;
+  d.n = h.size();
+  if (!h.empty()) e = cudaMemcpyAsync(d.ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+  return e;
+}
+
+template <class T>
+cudaError_t ensure(DevArray<T>& d, size_t n) {
+  if (d.n >= n && d.ptr) return cudaSuccess;
+  d.release();
+  cudaError_t const e = cudaMalloc(&d.ptr, (n ? n : 1) * sizeof(T));
+  if (e == cudaSuccess) d.n = n;
+  return e;
+}
+
+int bind_device(lgpu_ctx* ctx) {
+  cudaError_t const e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+  return LGPU_OK;
+}
+
+// Reads the device counters after a launch, updates the stats and reports
+// device-side checks.
+int collect(lgpu_ctx* ctx, const char* what) {
+  DevCounters c;
+  cudaError_t e = cudaMemcpyAsync(&c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_kernel_ms = ms;
+  ctx->stats.rays = c.rays;
+  ctx->stats.paths = c.paths;
+  ctx->stats.device_checks = c.flags;
+  ctx->stats.nonfinite_paths = c.nonfinite;
+  if (c.flags & 1u)
+    return fail(ctx, LGPU_ERR_DEVICE_CHECK,
+                std::string(what) + ": a traversal stack bound was exceeded; results are incomplete");
+  return LGPU_OK;
+}
+
+int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaStream_t st) {
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  RenderArgs a{};
+  a.spp = p->spp;
+  a.max_scatter = p->max_scatterings;
+  a.sample_p = p->sample_p;
+  a.flags = p->flags;
+  a.seed = p->seed;
+  a.spp_offset = p->spp_offset;
+  a.pixel_begin = 0;
+  a.pixel_count = uint32_t(ctx->S.cam.width * ctx->S.cam.height);
+  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
+  if (e == cudaSuccess) e = launch_render(ctx->S, a, d_out, ctx->counters, st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
+  return LGPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lgpu_abi_version(void) { return LGPU_ABI_VERSION; }
+
+int lgpu_create(int device, lgpu_ctx** out) {
+  if (!out) return LGPU_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return LGPU_ERR_NO_DEVICE;
+  if (device < 0 || device >= n) return LGPU_ERR_INVALID_ARGUMENT;
+  lgpu_ctx* ctx = new (std::nothrow) lgpu_ctx;
+  if (!ctx) return LGPU_ERR_OUT_OF_MEMORY;
+  ctx->device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, sizeof(DevCounters));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->exposure, sizeof(float));
+  if (e != cudaSuccess) {
+    lgpu_destroy(ctx);
+    return e == cudaErrorMemoryAllocation ? LGPU_ERR_OUT_OF_MEMORY : LGPU_ERR_CUDA;
+  }
+  *out = ctx;
+  return LGPU_OK;
+}
+
+void lgpu_destroy(lgpu_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->release_scene();
+  ctx->out.release();
+  ctx->rays.release();
+  ctx->hits.release();
+  ctx->partials.release();
+  ctx->tm_in.release();
+  ctx->tm_out.release();
+  ctx->tm_24.release();
+  if (ctx->counters) cudaFree(ctx->counters);
+  if (ctx->exposure) cudaFree(ctx->exposure);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* lgpu_last_error(const lgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int lgpu_upload_scene(lgpu_ctx* ctx, const lgpu_scene* scene) {
+  if (!ctx || !scene) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  HostLayout L;
+  std::string err;
+  int const rc = make_layout(*scene, L, err);
+  if (rc != LGPU_OK) return fail(ctx, rc, err);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->release_scene();
+  cudaStream_t const st = ctx->stream;
+  cudaError_t e = upload(ctx->objects, L.objects, st);
+  if (e == cudaSuccess) e = upload(ctx->meshes, L.meshes, st);
+  if (e == cudaSuccess) e = upload(ctx->nodes, L.nodes, st);
+  if (e == cudaSuccess) e = upload(ctx->tris, L.tris, st);
+  if (e == cudaSuccess) e = upload(ctx->shade, L.shade, st);
+  if (e == cudaSuccess) e = upload(ctx->spectra, L.spectra, st);
+  if (e == cudaSuccess) e = upload(ctx->mats, L.mats, st);
+  if (e == cudaSuccess) e = upload(ctx->lights, L.lights, st);
+  if (e == cudaSuccess) e = upload(ctx->tlas_objects, L.tlas_objects, st);
+  if (e == cudaSuccess) e = upload(ctx->cmf, L.cmf, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    ctx->release_scene();
+    return cuda_fail(ctx, e, "scene upload");
+  }
+  DevScene& S = ctx->S;
+  S = DevScene{};
+  S.objects = ctx->objects.ptr;
+  S.meshes = ctx->meshes.ptr;
+  S.nodes = ctx->nodes.ptr;
+  S.tris = ctx->tris.ptr;
+  S.shade = ctx->shade.ptr;
+  S.spectra = ctx->spectra.ptr;
+  S.mats = ctx->mats.ptr;
+  S.lights = ctx->lights.ptr;
+  S.tlas_objects = ctx->tlas_objects.ptr;
+  S.n_objects = scene->n_objects;
+  S.n_meshes = scene->n_meshes;
+  S.n_materials = scene->n_materials;
+  S.n_lights = scene->n_lights;
+  S.tlas_root = L.tlas_root;
+  S.max_stack = L.max_stack;
+  S.tlas_max_stack = L.tlas_max_stack;
+  S.n_bins = scene->spec.n_bins;
+  S.hero_k = scene->spec.hero_k;
+  S.lambda_inf = scene->spec.lambda_inf;
+  S.lambda_sup = scene->spec.lambda_sup;
+  // coefficientλ::Δ = (sup-inf)/(n-1) (cg.hpp:246)
+  S.lambda_delta = (S.lambda_sup - S.lambda_inf) / float(S.n_bins - 1);
+  S.cmf = ctx->cmf.ptr;
+  S.cam = scene->cam;
+  std::memcpy(S.tlas_bounds, L.tlas_bounds, sizeof(S.tlas_bounds));
+  ctx->stats.max_stack = L.max_stack;
+  ctx->has_scene = true;
+  return LGPU_OK;
+}
+
+int lgpu_render_device(lgpu_ctx* ctx, const lgpu_render_params* params, float* d_out, void* stream) {
+  if (!ctx || !d_out) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  int const rc = render_impl(ctx, params, d_out, st);
+  if (rc != LGPU_OK) return rc;
+  if (st != ctx->stream) {
+    cudaError_t const e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
+  }
+  return collect(ctx, "render");
+}
+
+int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linrgb) {
+  if (!ctx || !out_linrgb) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  size_t const n = size_t(ctx->S.cam.width) * ctx->S.cam.height * 3;
+  cudaError_t e = ensure(ctx->out, n);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "output buffer");
+  int const rc = render_impl(ctx, params, ctx->out.ptr, ctx->stream);
+  if (rc != LGPU_OK) return rc;
+  e = cudaMemcpyAsync(out_linrgb, ctx->out.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render readback");
+  return collect(ctx, "render");
+}
+
+int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {
+  if (!ctx || (n && (!rays || !out))) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  if (n == 0) return LGPU_OK;
+  cudaError_t e = ensure(ctx->rays, 6 * n);
+  if (e == cudaSuccess) e = ensure(ctx->hits, n);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "ray buffers");
+  cudaStream_t const st = ctx->stream;
+  e = cudaMemcpyAsync(ctx->rays.ptr, rays, 6 * n * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
+  if (e == cudaSuccess) e = launch_trace(ctx->S, ctx->rays.ptr, n, flags, ctx->hits.ptr, ctx->counters, st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, ctx->hits.ptr, n * sizeof(lgpu_hit), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "trace");
+  return collect(ctx, "trace");
+}
+
+int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h, float y_mid,
+                 float* out_tonemapped, uint8_t* out_rgb24) {
+  if (!ctx || !linrgb) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  uint64_t const n = w * h;
+  if (n == 0) return LGPU_OK;
+  cudaStream_t const st = ctx->stream;
+  uint32_t const nb = tonemap_partials_needed(n);
+  cudaError_t e = ensure(ctx->partials, nb);
+  if (e == cudaSuccess) e = ensure(ctx->tm_in, 3 * n);
+  if (e == cudaSuccess && out_tonemapped) e = ensure(ctx->tm_out, 3 * n);
+  if (e == cudaSuccess && out_rgb24) e = ensure(ctx->tm_24, 3 * n);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tone-map buffers");
+  e = cudaMemcpyAsync(ctx->tm_in.ptr, linrgb, 3 * n * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = launch_tonemap(ctx->tm_in.ptr, n, y_mid, ctx->partials.ptr, nb, ctx->exposure,
+                       out_tonemapped ? ctx->tm_out.ptr : nullptr, out_rgb24 ? ctx->tm_24.ptr : nullptr, st);
+  if (e == cudaSuccess && out_tonemapped)
+    e = cudaMemcpyAsync(out_tonemapped, ctx->tm_out.ptr, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && out_rgb24)
+    e = cudaMemcpyAsync(out_rgb24, ctx->tm_24.ptr, 3 * n, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "tone map");
+  return LGPU_OK;
+}
+
+int lgpu_get_stats(const lgpu_ctx* ctx, lgpu_stats* out) {
+  if (!ctx || !out) return LGPU_ERR_INVALID_ARGUMENT;
+  *out = ctx->stats;
+  return LGPU_OK;
+}
+
+int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F, uint32_t f_stride,
+                   uint32_t n_faces, uint32_t* nodes, uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
+                   uint32_t* prim_idxs, uint32_t* n_prim_idxs) {
+  if (!V || !F || f_stride < 3 || n_faces == 0 || !n_nodes || !n_bbs || !n_prim_idxs)
+    return LGPU_ERR_INVALID_ARGUMENT;
+  for (uint32_t f = 0; f < n_faces; f++)
+    for (int k = 0; k < 3; k++)
+      if (F[size_t(f) * f_stride + k] >= n_positions) return LGPU_ERR_INVALID_ARGUMENT;
+  try {
+    std::vector<PrimBox> boxes;
+    std::vector<float> cents;
+    triangle_prims(V, F, f_stride, n_faces, boxes, cents);
+    RefBvh B;
+    build_ref_bvh(n_faces, boxes.data(), cents.data(), B);
+    *n_nodes = B.n_nodes;
+    *n_bbs = uint32_t(B.bbs.size() / 48);
+    *n_prim_idxs = uint32_t(B.prim_idxs.size());
+    if (nodes) std::memcpy(nodes, B.nodes.data(), B.nodes.size() * sizeof(uint32_t));
+    if (bbs) std::memcpy(bbs, B.bbs.data(), B.bbs.size() * sizeof(float));
+    if (prim_idxs) std::memcpy(prim_idxs, B.prim_idxs.data(), B.prim_idxs.size() * sizeof(uint32_t));
+  } catch (const std::bad_alloc&) {
+    return LGPU_ERR_OUT_OF_MEMORY;
+  }
+  return LGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,53 @@
+// lgpu_layout.h — host-side construction of the device scene layout.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "lambda_gpu.h"
+#include "lgpu_scene.h"
+
+namespace lgpu {
+
+// Wide BVH in the reference's own format (cg.hpp:596-631), built with the
+// reference's algorithm (bvh::build, cg.hpp:632-749).
+struct RefBvh {
+  std::vector<uint32_t> nodes;  // pairs {childrenbb_idx, data}
+  std::vector<float> bbs;       // 48 floats per record
+  std::vector<uint32_t> prim_idxs;
+  uint32_t n_nodes = 0, n_interior = 0;
+};
+
+struct PrimBox {
+  float inf[3], sup[3];
+};
+
+// Builds over n primitives given their boxes and centroids
+// (centroid[3*i + axis]).
+void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out);
+
+// Boxes and centroids of triangle faces as trimeshdata::aabboftri and
+// centroidoftri compute them (cg.hpp:776-790).
+void triangle_prims(const float* V, const uint32_t* F, uint32_t f_stride, uint32_t n_faces,
+                    std::vector<PrimBox>& boxes, std::vector<float>& centroids);
+
+struct HostLayout {
+  std::vector<DevObject> objects;
+  std::vector<DevMesh> meshes;
+  std::vector<WideNode> nodes;
+  std::vector<TriSlot> tris;
+  std::vector<FaceShade> shade;
+  std::vector<float> spectra;
+  std::vector<DevMaterial> mats;
+  std::vector<lgpu_light> lights;
+  std::vector<uint32_t> tlas_objects;
+  std::vector<float> cmf;
+  uint32_t tlas_root = 0, max_stack = 0, tlas_max_stack = 0;
+  float tlas_bounds[6] = {0, 0, 0, 0, 0, 0};
+};
+
+// Validates the scene and lays it out for the device.  Returns LGPU_OK or
+// an lgpu_status with a message in err.
+int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err);
+
+}  // namespace lgpu

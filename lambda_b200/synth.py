@@ -1,0 +1,327 @@
+"""Seeded synthetic scenes for the benchmark configurations.
+
+Each generator writes a self-contained scene directory — scene.nls with
+absolute paths, triangle OBJ files with per-vertex normals, spectra as
+'λ,value' CSV files — that both the reference loader (load::loadNLS,
+cg.hpp:2455) and lambda_b200.scene.load_nls read.  The reference ships no
+benchmark scenes of these shapes; these stand in for them:
+
+  box_room   unit cube of 5 interior walls (10 triangles: white 0.75, left
+             0.6 above 600 nm / 0.05 below, right 0.6 in 500-560 nm / 0.05
+             elsewhere), two axis-aligned blocks (12 triangles each,
+             0.3x0.3x0.6 and 0.3x0.3x0.3, 0.75), a 0.25x0.25 ceiling quad
+             light with 6500 K blackbody emission.
+  instanced  N instances of one seeded displaced icosphere (subdivision s:
+             20*4^s triangles, Perlin displacement amplitude 0.05) on a
+             2-triangle ground plane under 2 quad lights; materials drawn
+             uniformly from Lambertian (smooth random spectra 0.05-0.9),
+             Blinn (exponent log-uniform 8-2048) and thin film (thickness
+             U[200,800] nm, IOR U[1.33,1.6]).
+"""
+import json
+import os
+
+import numpy as np
+
+from .scene import write_obj
+
+H_PLANCK = 6.62607015e-34
+C_LIGHT = 2.99792458e8
+K_BOLTZ = 1.380649e-23
+
+
+def planck(lam_nm, T):
+    lam = np.asarray(lam_nm, np.float64) * 1e-9
+    return 2 * H_PLANCK * C_LIGHT ** 2 / lam ** 5 / np.expm1(H_PLANCK * C_LIGHT / (lam * K_BOLTZ * T))
+
+
+def write_csv(path, lam, val):
+    with open(path, "w") as f:
+        for l, v in zip(lam, val):
+            f.write("%.1f,%.6f\n" % (l, v))
+
+
+def blackbody_csv(path, T, peak=1.0):
+    """Planck radiance at temperature T on 300-830 nm, scaled so that its
+    value at 560 nm is `peak`."""
+    lam = np.arange(300.0, 835.0, 5.0)
+    b = planck(lam, T)
+    b = b / planck([560.0], T)[0] * peak
+    write_csv(path, lam, b)
+
+
+def step_csv(path, lo, hi, inside, outside):
+    """inside on [lo, hi] nm, outside elsewhere, as a step sampled finely."""
+    lam, val = [], []
+    for l in np.arange(300.0, 835.0, 1.0):
+        lam.append(l)
+        val.append(inside if lo <= l <= hi else outside)
+    write_csv(path, lam, val)
+
+
+def smooth_random_csv(path, rng, lo=0.05, hi=0.9):
+    """A smooth random reflectance on 380-780 nm at 5 nm (81 samples):
+    a few random Gaussian bumps, rescaled into [lo, hi]."""
+    lam = np.arange(380.0, 785.0, 5.0)
+    v = np.zeros_like(lam)
+    for _ in range(3):
+        c = rng.uniform(380, 780)
+        w = rng.uniform(30, 120)
+        v += rng.uniform(0.2, 1.0) * np.exp(-0.5 * ((lam - c) / w) ** 2)
+    v = (v - v.min()) / max(v.max() - v.min(), 1e-6)
+    a, b = sorted(rng.uniform(lo, hi, size=2))
+    if b - a < 0.1:
+        b = min(hi, a + 0.1)
+    v = a + (b - a) * v
+    write_csv(path, lam, v)
+    return v
+
+
+def _quad(p0, p1, p2, p3):
+    """Two triangles of the quad p0 p1 p2 p3 (counter-clockwise seen from the
+    side its normal points to)."""
+    return [p0, p1, p2, p3], [(0, 1, 2), (0, 2, 3)]
+
+
+def _write_flat_mesh(path, quads):
+    """OBJ of planar quads with one flat normal per quad: normal = (p1-p0) x
+    (p2-p0), the geometric normal the reference loader computes."""
+    V, N, F = [], [], []
+    for q in quads:
+        base = len(V)
+        p = [np.asarray(x, np.float64) for x in q]
+        n = np.cross(p[1] - p[0], p[2] - p[0])
+        n /= np.linalg.norm(n)
+        V.extend(p)
+        N.append(n)
+        ni = len(N)
+        F.append((base + 1, base + 2, base + 3, ni, ni, ni))
+        F.append((base + 1, base + 3, base + 4, ni, ni, ni))
+    write_obj(path, V, N, F)
+
+
+def _box_quads(lo, hi, inward=False):
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    quads = [
+        [(x0, y0, z0), (x0, y1, z0), (x1, y1, z0), (x1, y0, z0)],  # bottom (-z)
+        [(x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1)],  # top (+z)
+        [(x0, y0, z0), (x1, y0, z0), (x1, y0, z1), (x0, y0, z1)],  # front (-y)
+        [(x0, y1, z0), (x0, y1, z1), (x1, y1, z1), (x1, y1, z0)],  # back (+y)
+        [(x0, y0, z0), (x0, y0, z1), (x0, y1, z1), (x0, y1, z0)],  # left (-x)
+        [(x1, y0, z0), (x1, y1, z0), (x1, y1, z1), (x1, y0, z1)],  # right (+x)
+    ]
+    if inward:
+        quads = [q[::-1] for q in quads]
+    return quads
+
+
+def _mat_spec(path):
+    return {"val": path}
+
+
+def box_room(out_dir, width=256, light_peak=6.0):
+    """Writes the box-room scene; returns the .nls path."""
+    os.makedirs(out_dir, exist_ok=True)
+    d = os.path.abspath(out_dir)
+    walls = _box_quads((0, 0, 0), (1, 1, 1), inward=True)
+    # inward walls: bottom, top, back, left, right (the -y side is open)
+    white = [walls[0], walls[1], walls[3]]
+    _write_flat_mesh(os.path.join(d, "walls_white.obj"), white)
+    _write_flat_mesh(os.path.join(d, "wall_left.obj"), [walls[4]])
+    _write_flat_mesh(os.path.join(d, "wall_right.obj"), [walls[5]])
+    _write_flat_mesh(os.path.join(d, "block_tall.obj"),
+                     _box_quads((0.2, 0.45, 0.0), (0.5, 0.75, 0.6)))
+    _write_flat_mesh(os.path.join(d, "block_short.obj"),
+                     _box_quads((0.58, 0.2, 0.0), (0.88, 0.5, 0.3)))
+    step_csv(os.path.join(d, "left.csv"), 600.0, 10000.0, 0.6, 0.05)
+    step_csv(os.path.join(d, "right.csv"), 500.0, 560.0, 0.6, 0.05)
+    blackbody_csv(os.path.join(d, "bb6500.csv"), 6500.0, light_peak)
+    scene = {
+        "camera": {"pos": [0.5, -1.4, 0.5], "look_at": [0.5, 0.5, 0.5], "up": [0, 0, 1],
+                   "fov": 40, "ar": 1.0, "width": width},
+        "materials": [
+            {"name": "white", "type": "lambertian", "albedo": {"val": 0.75}},
+            {"name": "left", "type": "lambertian", "albedo": _mat_spec(os.path.join(d, "left.csv"))},
+            {"name": "right", "type": "lambertian",
+             "albedo": _mat_spec(os.path.join(d, "right.csv"))},
+        ],
+        "objects": [
+            {"name": "walls", "type": "trimesh", "transform": {},
+             "material": "white", "source": os.path.join(d, "walls_white.obj")},
+            {"name": "left", "type": "trimesh", "transform": {},
+             "material": "left", "source": os.path.join(d, "wall_left.obj")},
+            {"name": "right", "type": "trimesh", "transform": {},
+             "material": "right", "source": os.path.join(d, "wall_right.obj")},
+            {"name": "tall", "type": "trimesh", "transform": {},
+             "material": "white", "source": os.path.join(d, "block_tall.obj")},
+            {"name": "short", "type": "trimesh", "transform": {},
+             "material": "white", "source": os.path.join(d, "block_short.obj")},
+        ],
+        "lights": [
+            {"name": "ceiling", "type": "quaddir", "specular": 1,
+             "transform": {"scale": [0.125, 0.125, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                           "translate": [0.5, 0.5, 0.998]},
+             "radiance": {"val": os.path.join(d, "bb6500.csv")}},
+        ],
+    }
+    path = os.path.join(d, "scene.nls")
+    with open(path, "w") as f:
+        json.dump(scene, f, indent=1)
+    return path
+
+
+# ---- displaced icosphere ---------------------------------------------------------
+
+def icosphere(subdiv):
+    """Unit icosphere: 20*4^subdiv triangles, outward winding."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    V = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t),
+         (0, 1, -t), (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    F = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4),
+         (11, 10, 2), (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9),
+         (4, 9, 5), (2, 4, 11), (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    V = np.array(V, np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array(F, np.int64)
+    for _ in range(subdiv):
+        nv = V.shape[0]
+        e = np.concatenate([F[:, [0, 1]], F[:, [1, 2]], F[:, [2, 0]]])
+        key = np.minimum(e[:, 0], e[:, 1]) * (nv + 1) + np.maximum(e[:, 0], e[:, 1])
+        uniq, inv = np.unique(key, return_inverse=True)
+        a = uniq // (nv + 1)
+        b = uniq % (nv + 1)
+        mid = V[a] + V[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        mids = nv + inv.reshape(3, -1).T  # (n_faces, 3): m01, m12, m20
+        V = np.concatenate([V, mid])
+        f0, f1, f2 = F[:, 0], F[:, 1], F[:, 2]
+        m01, m12, m20 = mids[:, 0], mids[:, 1], mids[:, 2]
+        F = np.concatenate([np.stack([f0, m01, m20], 1), np.stack([f1, m12, m01], 1),
+                            np.stack([f2, m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    return V, F
+
+
+def perlin3(p, perm):
+    """Improved Perlin noise (Perlin 2002) at points p (n, 3)."""
+    def fade(t):
+        return t * t * t * (t * (t * 6 - 15) + 10)
+
+    def grad(h, x, y, z):
+        h = h & 15
+        u = np.where(h < 8, x, y)
+        v = np.where(h < 4, y, np.where((h == 12) | (h == 14), x, z))
+        return np.where(h & 1, -u, u) + np.where(h & 2, -v, v)
+
+    P = np.floor(p).astype(np.int64)
+    f = p - P
+    X, Y, Z = (P[:, 0] & 255), (P[:, 1] & 255), (P[:, 2] & 255)
+    x, y, z = f[:, 0], f[:, 1], f[:, 2]
+    u, v, w = fade(x), fade(y), fade(z)
+    pp = np.concatenate([perm, perm])
+    A = pp[X] + Y
+    AA, AB = pp[A] + Z, pp[A + 1] + Z
+    B = pp[X + 1] + Y
+    BA, BB = pp[B] + Z, pp[B + 1] + Z
+
+    def lerp(t, a, b):
+        return a + t * (b - a)
+
+    return lerp(w, lerp(v, lerp(u, grad(pp[AA], x, y, z), grad(pp[BA], x - 1, y, z)),
+                        lerp(u, grad(pp[AB], x, y - 1, z), grad(pp[BB], x - 1, y - 1, z))),
+                lerp(v, lerp(u, grad(pp[AA + 1], x, y, z - 1), grad(pp[BA + 1], x - 1, y, z - 1)),
+                     lerp(u, grad(pp[AB + 1], x, y - 1, z - 1), grad(pp[BB + 1], x - 1, y - 1, z - 1))))
+
+
+def displaced_icosphere(subdiv, seed, amp=0.05, freq=3.0):
+    """Icosphere displaced along its normal by amp * Perlin(freq * p); vertex
+    normals are area-weighted face normals of the displaced surface."""
+    V, F = icosphere(subdiv)
+    rng = np.random.default_rng(seed)
+    perm = rng.permutation(256)
+    n = perlin3(V * freq + rng.uniform(0, 100, size=3), perm)
+    V = V * (1.0 + amp * n)[:, None]
+    e0 = V[F[:, 1]] - V[F[:, 0]]
+    e2 = V[F[:, 2]] - V[F[:, 0]]
+    fn = np.cross(e0, e2)
+    N = np.zeros_like(V)
+    for k in range(3):
+        np.add.at(N, F[:, k], fn)
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    return V, N, F
+
+
+def write_indexed_obj(path, V, N, F):
+    """OBJ with shared vertices: face corner k uses position and normal k."""
+    Fo = np.concatenate([F + 1, F + 1], axis=1)
+    write_obj(path, V, N, Fo)
+
+
+def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 9):
+    """Writes the instanced scene; returns the .nls path."""
+    os.makedirs(out_dir, exist_ok=True)
+    d = os.path.abspath(out_dir)
+    rng = np.random.default_rng(seed)
+    mesh_path = os.path.join(d, f"icosphere_s{subdiv}_seed{seed}.obj")
+    if not os.path.exists(mesh_path):
+        V, N, F = displaced_icosphere(subdiv, seed)
+        write_indexed_obj(mesh_path, V, N, F)
+    _write_flat_mesh(os.path.join(d, "ground.obj"),
+                     [[(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)]])
+    blackbody_csv(os.path.join(d, "bb6500.csv"), 6500.0, 3.0)
+    blackbody_csv(os.path.join(d, "bb4000.csv"), 4000.0, 2.0)
+    materials = [{"name": "ground", "type": "lambertian", "albedo": {"val": 0.5}}]
+    objects = [{"name": "ground", "type": "trimesh", "material": "ground",
+                "transform": {"scale": [12, 12, 1]}, "source": os.path.join(d, "ground.obj")}]
+    side = int(np.ceil(np.sqrt(n_instances)))
+    spacing = 1.1
+    for i in range(n_instances):
+        kind = ["lambertian", "blinn", "thinfilm"][int(rng.integers(0, 3))]
+        name = f"m{i}"
+        if kind == "lambertian":
+            p = os.path.join(d, f"albedo_{i}.csv")
+            smooth_random_csv(p, rng)
+            materials.append({"name": name, "type": "lambertian", "albedo": {"val": p}})
+        elif kind == "blinn":
+            p = os.path.join(d, f"kd_{i}.csv")
+            smooth_random_csv(p, rng, 0.05, 0.6)
+            # an even integer exponent keeps powf defined for back-facing
+            # half vectors (cg.hpp:1810, 1822)
+            alpha = 2 * int(round(np.exp(rng.uniform(np.log(8), np.log(2048))) / 2))
+            materials.append({"name": name, "type": "blinn", "Kd": {"val": p},
+                              "Ks": {"val": float(rng.uniform(0.2, 0.5))}, "glossiness": alpha})
+        else:
+            alpha = 2 * int(round(np.exp(rng.uniform(np.log(8), np.log(2048))) / 2))
+            materials.append({"name": name, "type": "thinfilm",
+                              "film_ior": {"val": float(rng.uniform(1.33, 1.6))},
+                              "base_ior": {"val": 1.5}, "glossiness": alpha,
+                              "thickness": float(rng.uniform(200, 800))})
+        gx, gy = i % side, i // side
+        s = 0.45
+        objects.append({"name": f"inst{i}", "type": "trimesh", "material": name,
+                        "source": mesh_path,
+                        "transform": {"scale": [s, s, s],
+                                      "rotate": {"axis": [0, 0, 1],
+                                                 "degrees": float(rng.uniform(0, 360))},
+                                      "translate": [(gx - (side - 1) / 2) * spacing,
+                                                    (gy - (side - 1) / 2) * spacing, s]}})
+    lights = [
+        {"name": "key", "type": "quaddir", "specular": 1,
+         "transform": {"scale": [1.5, 1.5, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [-2.0, -1.0, 6.0]},
+         "radiance": {"val": os.path.join(d, "bb6500.csv")}},
+        {"name": "fill", "type": "quaddir", "specular": 1,
+         "transform": {"scale": [1.0, 1.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [3.0, 2.0, 5.0]},
+         "radiance": {"val": os.path.join(d, "bb4000.csv")}},
+    ]
+    extent = side * spacing
+    scene = {
+        "camera": {"pos": [0.0, -0.95 * extent, 0.75 * extent], "look_at": [0, 0, 0.2],
+                   "up": [0, 0, 1], "fov": 50, "ar": ar, "width": width},
+        "materials": materials, "objects": objects, "lights": lights,
+    }
+    path = os.path.join(d, "scene.nls")
+    with open(path, "w") as f:
+        json.dump(scene, f, indent=1)
+    return path
