@@ -1,0 +1,148 @@
+"""Renderer — the Python host's mirror of the reference's Renderer class
+(include/renderer.hpp:32-52) on top of the C ABI.
+
+    r = Renderer()                 # MAX_SCATTERINGS=4, SPP=4, SAMPLE_P=0.5
+    r.SPP, r.MAX_SCATTERINGS, r.SAMPLE_P = 16, 8, 0.8
+    buf = Rendering()
+    r.render(scene, buf)           # Renderer::render, src/renderer.cpp:14
+    tm = Rendering()
+    r.toneMap(buf, tm, 0.12)       # Renderer::toneMap, src/renderer.cpp:149
+    rgb8 = tm.rgb24()              # rendering::rgb24, include/renderer.hpp:20
+
+Rendering runs on the GPU through liblambda_gpu.so; there is no CPU path.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .scene import FlatScene, SceneData
+
+
+class Rendering:
+    """rendering (include/renderer.hpp:16-30): img is (height, width, 3)
+    linear RGB float32, row 0 at the top."""
+
+    def __init__(self, img=None):
+        self.img = img
+
+    def rgb24(self, ctx=None):
+        """8-bit sRGB of img (linRGB2sRGB then float2byte, cg.hpp:149-162)."""
+        x = self.img.astype(np.float32)
+        s = np.where(x > np.float32(0.0031308),
+                     np.float32(1.055) * np.power(x, np.float32(1 / 2.4)) - np.float32(0.055),
+                     np.float32(12.92) * x)
+        return np.clip((np.float32(255) * s + np.float32(0.5)).astype(np.int64), 0, 255).astype(np.uint8)
+
+
+class Context:
+    """One lgpu_ctx (one CUDA device, one uploaded scene)."""
+
+    def __init__(self, device=0):
+        self._lib = L.lib()
+        h = ctypes.c_void_p()
+        rc = self._lib.lgpu_create(int(device), ctypes.byref(h))
+        L.check(None, rc, "lgpu_create")
+        self.h = h
+        self.flat = None
+        self._scene_id = None
+
+    def close(self):
+        if self.h:
+            self._lib.lgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, scene):
+        flat = scene if isinstance(scene, FlatScene) else FlatScene(scene)
+        L.check(self.h, self._lib.lgpu_upload_scene(self.h, flat.ptr()), "upload")
+        self.flat = flat
+        self._scene_id = id(scene)
+        return flat
+
+    @property
+    def size(self):
+        c = self.flat.scene.cam
+        return int(c.width), int(c.height)
+
+    def render(self, spp, max_scatterings, sample_p, seed=0, flags=0, spp_offset=0, out=None):
+        w, h = self.size
+        if out is None:
+            out = np.empty((h, w, 3), np.float32)
+        p = L.RenderParams(spp=spp, max_scatterings=max_scatterings, sample_p=sample_p, flags=flags,
+                           seed=seed, spp_offset=spp_offset)
+        L.check(self.h, self._lib.lgpu_render(self.h, ctypes.byref(p), out.ctypes.data), "render")
+        return out
+
+    def render_device(self, spp, max_scatterings, sample_p, d_out_ptr, seed=0, flags=0,
+                      spp_offset=0, stream=None):
+        p = L.RenderParams(spp=spp, max_scatterings=max_scatterings, sample_p=sample_p, flags=flags,
+                           seed=seed, spp_offset=spp_offset)
+        L.check(self.h, self._lib.lgpu_render_device(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr),
+                                                     ctypes.c_void_p(stream or 0)), "render_device")
+
+    def trace(self, rays, flags=0):
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        out = (L.Hit * max(rays.shape[0], 1))()
+        L.check(self.h, self._lib.lgpu_trace_closest(self.h, rays.ctypes.data, rays.shape[0], flags,
+                                                     ctypes.addressof(out)), "trace")
+        return hits_to_numpy(out, rays.shape[0])
+
+    def tonemap(self, linrgb, y_mid=0.12):
+        img = np.ascontiguousarray(linrgb, np.float32)
+        h, w = img.shape[:2]
+        tm = np.empty_like(img)
+        b = np.empty(img.shape, np.uint8)
+        L.check(self.h, self._lib.lgpu_tonemap(self.h, img.ctypes.data, w, h, y_mid, tm.ctypes.data,
+                                               b.ctypes.data), "tonemap")
+        return tm, b
+
+    def stats(self):
+        s = L.Stats()
+        L.check(self.h, self._lib.lgpu_get_stats(self.h, ctypes.byref(s)), "stats")
+        return {"last_kernel_ms": s.last_kernel_ms, "rays": s.rays, "paths": s.paths,
+                "device_checks": s.device_checks, "max_stack": s.max_stack,
+                "nonfinite_paths": s.nonfinite_paths}
+
+
+def hits_to_numpy(arr, n):
+    """lgpu_hit array -> structured numpy array."""
+    dt = np.dtype([("t", np.float32), ("obj", np.uint32), ("face", np.uint32), ("mat", np.uint32),
+                   ("p", np.float32, 3), ("n", np.float32, 3), ("gn", np.float32, 3),
+                   ("front", np.uint32)])
+    assert dt.itemsize == ctypes.sizeof(L.Hit)
+    buf = np.frombuffer(ctypes.string_at(ctypes.addressof(arr), n * dt.itemsize), dtype=dt)
+    return buf.copy()
+
+
+class Renderer:
+    """Renderer (include/renderer.hpp:32-52).  render() uploads the scene
+    when it is not the one uploaded last, then renders on the device."""
+
+    def __init__(self, device=0, seed=0, flags=0):
+        self.MAX_SCATTERINGS = 4
+        self.SPP = 4
+        self.SAMPLE_P = 0.5
+        self.seed = seed
+        self.flags = flags
+        self.ctx = Context(device)
+
+    def render(self, scene, buffer):
+        if self.ctx._scene_id != id(scene):
+            self.ctx.upload(scene)
+        buffer.img = self.ctx.render(int(self.SPP), int(self.MAX_SCATTERINGS), float(self.SAMPLE_P),
+                                     seed=self.seed, flags=self.flags)
+        return buffer
+
+    def toneMap(self, buffer, tm_buffer, Y_MID=0.12):
+        tm, _ = self.ctx.tonemap(buffer.img, Y_MID)
+        tm_buffer.img = tm
+        return tm_buffer
+
+    def tracePath(self, *args, **kwargs):
+        raise NotImplementedError("single paths are traced inside the render kernel")

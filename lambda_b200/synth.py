@@ -159,7 +159,7 @@ def box_room(out_dir, width=256, light_peak=6.0):
              "material": "white", "source": os.path.join(d, "block_short.obj")},
         ],
         "lights": [
-            {"name": "ceiling", "type": "quaddir", "specular": 1,
+            {"name": "ceiling", "type": "quaddir", "specular": 2,
              "transform": {"scale": [0.125, 0.125, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
                            "translate": [0.5, 0.5, 0.998]},
              "radiance": {"val": os.path.join(d, "bb6500.csv")}},
@@ -257,6 +257,79 @@ def write_indexed_obj(path, V, N, F):
     write_obj(path, V, N, Fo)
 
 
+def mixed(out_dir, width=96, ar=1.25, lights=("sphere", "quaddir", "point"), seed=7,
+          subdiv=3):
+    """A small scene with every object kind (sphere, plane, instanced
+    trimesh), every shaded material (Lambertian, Blinn reflective/diffuse,
+    Blinn refractive with a dispersive IOR, thin film) and the requested
+    light kinds (sphere, quaddir, point, direction, ambient).  Returns the
+    .nls path."""
+    os.makedirs(out_dir, exist_ok=True)
+    d = os.path.abspath(out_dir)
+    rng = np.random.default_rng(seed)
+    mesh = os.path.join(d, f"ico_s{subdiv}.obj")
+    V, N, F = displaced_icosphere(subdiv, seed, amp=0.08)
+    write_indexed_obj(mesh, V, N, F)
+    smooth_random_csv(os.path.join(d, "albedo.csv"), rng, 0.1, 0.8)
+    blackbody_csv(os.path.join(d, "bb.csv"), 5000.0, 4.0)
+    lam = np.arange(330.0, 800.0, 10.0)
+    write_csv(os.path.join(d, "glass_ior.csv"), lam, 1.5 + 4000.0 / lam ** 2)
+    write_csv(os.path.join(d, "film_ior.csv"), lam, 1.35 + 2000.0 / lam ** 2)
+    mats = [
+        {"name": "floor", "type": "lambertian", "albedo": {"val": [0.6, 0.55, 0.5]}},
+        {"name": "wall", "type": "lambertian", "albedo": {"val": os.path.join(d, "albedo.csv")}},
+        {"name": "gloss", "type": "blinn", "Kd": {"val": [0.7, 0.3, 0.1]}, "Ks": {"val": 0.3},
+         "glossiness": 64},
+        {"name": "mirror", "type": "blinn", "Ks": {"val": 0.9}, "glossiness": 512},
+        {"name": "glass", "type": "blinn", "Kt": {"val": 0.9}, "Kd": {"val": 0.02},
+         "glossiness": 2048, "ior": {"val": os.path.join(d, "glass_ior.csv")}},
+        {"name": "film", "type": "thinfilm", "glossiness": 256, "thickness": 480,
+         "film_ior": {"val": os.path.join(d, "film_ior.csv")}, "base_ior": {"val": 1.6}},
+    ]
+    objs = [
+        {"name": "floor", "type": "plane", "transform": {"scale": [8, 8, 1]}, "material": "floor"},
+        {"name": "back", "type": "plane", "material": "wall",
+         "transform": {"scale": [8, 4, 1], "rotate": {"axis": [1, 0, 0], "degrees": 90},
+                       "translate": [0, 3, 4]}},
+        {"name": "ball", "type": "sphere", "material": "gloss",
+         "transform": {"scale": [0.8, 0.8, 0.8], "translate": [-1.6, 0.2, 0.8]}},
+        {"name": "chrome", "type": "sphere", "material": "mirror",
+         "transform": {"scale": [0.6, 0.6, 0.6], "translate": [1.7, 1.0, 0.6]}},
+        {"name": "rock1", "type": "trimesh", "material": "glass", "source": mesh,
+         "transform": {"scale": [0.9, 0.9, 0.9], "rotate": {"axis": [0, 1, 1], "degrees": 30},
+                       "translate": [0.1, -0.4, 0.9]}},
+        {"name": "rock2", "type": "trimesh", "material": "film", "source": mesh,
+         "transform": {"scale": [0.7, 0.5, 0.7], "rotate": {"axis": [1, 0, 0], "degrees": -20},
+                       "translate": [1.2, -1.3, 0.5]}},
+    ]
+    ls = []
+    for kind in lights:
+        if kind == "sphere":
+            ls.append({"name": "sun", "type": "sphere", "radiance": {"val": 6.0},
+                       "transform": {"scale": [0.5, 0.5, 0.5], "translate": [-2.5, -1.5, 4.0]}})
+        elif kind == "quaddir":
+            ls.append({"name": "panel", "type": "quaddir", "specular": 2,
+                       "radiance": {"val": os.path.join(d, "bb.csv")},
+                       "transform": {"scale": [0.8, 0.6, 1],
+                                     "rotate": {"axis": [1, 0, 0], "degrees": 160},
+                                     "translate": [1.5, -0.5, 3.5]}})
+        elif kind == "point":
+            ls.append({"name": "bulb", "type": "point", "radiant_intensity": {"val": 3.0},
+                       "pos": [0.5, -2.5, 2.5]})
+        elif kind == "direction":
+            ls.append({"name": "sky", "type": "direction", "radiant_intensity": {"val": 0.8},
+                       "dir": [0.3, 0.4, -0.866]})
+        elif kind == "ambient":
+            ls.append({"name": "amb", "type": "ambient", "radiance": {"val": 0.15}})
+    scene = {"camera": {"pos": [0.0, -6.0, 2.2], "look_at": [0.0, 0.0, 0.8], "up": [0, 0, 1],
+                        "fov": 45, "ar": ar, "width": width},
+             "materials": mats, "objects": objs, "lights": ls}
+    path = os.path.join(d, "scene.nls")
+    with open(path, "w") as f:
+        json.dump(scene, f, indent=1)
+    return path
+
+
 def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 9):
     """Writes the instanced scene; returns the .nls path."""
     os.makedirs(out_dir, exist_ok=True)
@@ -306,11 +379,11 @@ def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 
                                       "translate": [(gx - (side - 1) / 2) * spacing,
                                                     (gy - (side - 1) / 2) * spacing, s]}})
     lights = [
-        {"name": "key", "type": "quaddir", "specular": 1,
+        {"name": "key", "type": "quaddir", "specular": 2,
          "transform": {"scale": [1.5, 1.5, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
                        "translate": [-2.0, -1.0, 6.0]},
          "radiance": {"val": os.path.join(d, "bb6500.csv")}},
-        {"name": "fill", "type": "quaddir", "specular": 1,
+        {"name": "fill", "type": "quaddir", "specular": 2,
          "transform": {"scale": [1.0, 1.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
                        "translate": [3.0, 2.0, 5.0]},
          "radiance": {"val": os.path.join(d, "bb4000.csv")}},
