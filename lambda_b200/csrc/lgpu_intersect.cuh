@@ -123,10 +123,17 @@ struct HitRec {
   uint32_t face;  // trimesh face, UINT32_MAX otherwise
   float b0, b1, b2;
   f3 pl;  // local-space hit point
+  // for the instance-BVH order: the hit object's bounds contained the ray
+  // origin, and the distance at which the ray leaves them
+  bool inside;
+  float exit;
 };
 
-// intersect::aabb (cg.hpp:1268-1286): scalar slab test for mesh bounds
-__device__ __forceinline__ float aabb_scalar(const float* bb, const Ray& r, float t_max) {
+// intersect::aabb (cg.hpp:1268-1286): scalar slab test for mesh bounds.
+// When the origin is inside the box (tmin < BIAS) it returns the exit
+// distance; `inside` and `exit_t` report that case.
+__device__ __forceinline__ float aabb_scalar(const float* bb, const Ray& r, float t_max, bool& inside,
+                                             float& exit_t) {
   float t0x = ml(sb(bb[0], r.p.x), r.inv.x);
   float t1x = ml(sb(bb[3], r.p.x), r.inv.x);
   float t0y = ml(sb(bb[1], r.p.y), r.inv.y);
@@ -141,8 +148,31 @@ __device__ __forceinline__ float aabb_scalar(const float* bb, const Ray& r, floa
   float const tmin = t0x >= myz ? t0x : myz;
   float const nyz = t1y <= t1z ? t1y : t1z;
   float const tmax = t1x <= nyz ? t1x : nyz;
+  inside = false;
+  exit_t = tmax;
   if (tmax < kBias || tmax <= tmin || tmin > t_max) return kFltMax;
-  return tmin < kBias ? tmax : tmin;
+  inside = tmin < kBias;
+  return inside ? tmax : tmin;
+}
+
+// Entry distance of the ray segment [BIAS, t_max] into a box, or FLT_MAX if
+// the segment misses it (conservative culling for the instance BVH root).
+__device__ __forceinline__ float segment_box_entry(const float* bb, const Ray& r, float t_max) {
+  float tmin = kBias, tmax = t_max;
+  float const a[3] = {r.p.x, r.p.y, r.p.z}, iv[3] = {r.inv.x, r.inv.y, r.inv.z};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float t0 = ml(sb(bb[k], a[k]), iv[k]);
+    float t1 = ml(sb(bb[3 + k], a[k]), iv[k]);
+    if (t0 > t1) { float s = t0; t0 = t1; t1 = s; }
+    tmin = t0 > tmin ? t0 : tmin;
+    tmax = t1 < tmax ? t1 : tmax;
+  }
+  return tmin <= tmax ? tmin : kFltMax;
+}
+
+__device__ __forceinline__ float prev_float(float z) {
+  return __int_as_float(__float_as_int(z) - 1);
 }
 
 // intersect::aabb_avx2 (cg.hpp:1295-1337) for child c of a wide node:
@@ -277,20 +307,32 @@ __device__ __forceinline__ bool plane_test(const Ray& l, float z, float& t_out, 
   return true;
 }
 
-struct TraverseStatus {
-  uint32_t overflow;  // a push would have exceeded the stack
-};
+// Traversal orders.  kRefOrder reproduces intersect::scene's linear object
+// loop; kTlasClosest / kTlasAny visit objects through the instance BVH.
+enum Order { kRefOrder = 0, kTlasClosest = 1, kTlasAny = 2 };
 
 // intersect::trimesh (cg.hpp:1382-1460) on one instance; ANY stops at the
 // first accepted triangle (shadow rays only need the boolean).
+//
+// The reference pushes the mesh root with the value intersect::aabb returns,
+// which is the box's EXIT distance when the ray starts inside the bounds;
+// the root is then skipped if that exit lies beyond the closest hit so far
+// (cg.hpp:1393, 1414).  Hits inside such a mesh are lost depending on which
+// objects were tested before it.  kRefOrder and the shadow-ray orders keep
+// that rule as is.  kTlasClosest tests such a mesh in full and records in
+// the hit that it was an inside-bounds object, so that scene_hit can detect
+// when the reference's object order could have changed the answer.
 template <bool ANY>
 __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, const DevObject& ob,
                                             const Ray& w, HitRec& h, StackEntry* stack,
-                                            uint32_t& flags) {
+                                            uint32_t& flags, int order) {
   Ray const l = to_local(ob, w);
   const DevMesh& m = S.meshes[ob.mesh];
-  float const t0 = aabb_scalar(m.bounds, l, h.z);
+  bool inside;
+  float exit_t;
+  float t0 = aabb_scalar(m.bounds, l, h.z, inside, exit_t);
   if (t0 == kFltMax) return false;
+  if (order == kTlasClosest && inside) t0 = kBias;
   f3 const mr = cross3(l.p, l.u);
   int sp = 0;
   stack[sp++] = StackEntry{m.root, t0};
@@ -319,6 +361,8 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
         h.b1 = b1;
         h.b2 = b2;
         h.pl = ray_at(l, t);
+        h.inside = inside;
+        h.exit = exit_t;
         hit_any = true;
         if (ANY) return true;
       }
@@ -329,9 +373,9 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
 
 template <bool ANY>
 __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const Ray& w, HitRec& h,
-                                           StackEntry* stack, uint32_t& flags) {
+                                           StackEntry* stack, uint32_t& flags, int order) {
   const DevObject& ob = S.objects[i];
-  if (ob.type == LGPU_OBJ_TRIMESH) return trimesh_hit<ANY>(S, i, ob, w, h, stack, flags);
+  if (ob.type == LGPU_OBJ_TRIMESH) return trimesh_hit<ANY>(S, i, ob, w, h, stack, flags, order);
   Ray const l = to_local(ob, w);
   float t;
   if (ob.type == LGPU_OBJ_SPHERE) {
@@ -340,6 +384,7 @@ __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const 
     h.obj = i;
     h.face = UINT32_MAX;
     h.pl = ray_at(l, t);
+    h.inside = false;
     return true;
   }
   f3 x;
@@ -348,51 +393,79 @@ __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const 
   h.obj = i;
   h.face = UINT32_MAX;
   h.pl = x;
+  h.inside = false;
   return true;
 }
 
-// intersect::scene (cg.hpp:1469-1489).  With reference_order the objects are
-// tested in index order like the reference; otherwise an instance-level BVH
-// selects them (same hits; only exact ties between objects may resolve to a
-// different object).  `skip` is an object index to ignore.
+// intersect::scene (cg.hpp:1469-1489).  `skip` is an object index to ignore.
+//
+// With reference_order the objects are tested in index order like the
+// reference.  Otherwise an instance-level BVH selects them, and the result
+// is made identical to the index-order loop: on equal distances the object
+// with the higher index wins (later objects overwrite ties, cg.hpp:1214,
+// 1251, 1368), and when the winner is a mesh whose bounds contain the ray
+// origin with an exit beyond the hit — the only case where the reference's
+// answer depends on the object order — the ray is re-traced in index order.
+// Shadow rays (ANY) need neither: the reference's per-object rule with the
+// initial distance decides them in any order.
 template <bool ANY>
 __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRec& h, uint32_t skip,
                                           bool reference_order, StackEntry* stack,
                                           StackEntry* tstack, uint32_t& flags) {
-  bool hit_any = false;
+  h.inside = false;
   if (reference_order || S.n_objects <= 4) {
+    bool hit_any = false;
     for (uint32_t i = 0; i < S.n_objects; i++) {
       if (i == skip) continue;
-      if (object_hit<ANY>(S, i, w, h, stack, flags)) {
+      if (object_hit<ANY>(S, i, w, h, stack, flags, kRefOrder)) {
         hit_any = true;
         if (ANY) return true;
       }
     }
     return hit_any;
   }
-  float const t0 = aabb_scalar(S.tlas_bounds, w, h.z);
-  if (t0 == kFltMax) return false;
-  int sp = 0;
-  tstack[sp++] = StackEntry{S.tlas_root, t0};
-  while (sp > 0) {
-    StackEntry const e = tstack[--sp];
-    if (e.t > h.z) continue;
-    if (!(e.ref & kLeafBit)) {
-      if (!push_children(S.nodes[e.ref], w, h.z, tstack, sp, kTlasStackCap)) {
-        flags |= 1u;
-        break;
+  int const order = ANY ? kTlasAny : kTlasClosest;
+  HitRec const h0 = h;
+  bool hit_any = false;
+  float const t0 = segment_box_entry(S.tlas_bounds, w, h.z);
+  if (t0 != kFltMax) {
+    int sp = 0;
+    tstack[sp++] = StackEntry{S.tlas_root, t0};
+    while (sp > 0) {
+      StackEntry const e = tstack[--sp];
+      if (e.t > h.z) continue;
+      if (!(e.ref & kLeafBit)) {
+        if (!push_children(S.nodes[e.ref], w, h.z, tstack, sp, kTlasStackCap)) {
+          flags |= 1u;
+          break;
+        }
+        continue;
       }
-      continue;
+      uint32_t const count = ((e.ref >> 28) & 7u) + 1u;
+      uint32_t const slot = e.ref & kSlotMask;
+      for (uint32_t k = 0; k < count; k++) {
+        uint32_t const i = S.tlas_objects[slot + k];
+        if (i == skip) continue;
+        if (ANY) {
+          if (object_hit<true>(S, i, w, h, stack, flags, order)) return true;
+          continue;
+        }
+        // a lower-index object loses ties: test it against the next float
+        // below the current distance
+        float const zs = h.z;
+        bool const lowered = (h.obj != UINT32_MAX && i < h.obj);
+        if (lowered) h.z = prev_float(zs);
+        if (object_hit<false>(S, i, w, h, stack, flags, order)) hit_any = true;
+        else if (lowered) h.z = zs;
+      }
     }
-    uint32_t const count = ((e.ref >> 28) & 7u) + 1u;
-    uint32_t const slot = e.ref & kSlotMask;
-    for (uint32_t k = 0; k < count; k++) {
-      uint32_t const i = S.tlas_objects[slot + k];
+  }
+  if (!ANY && hit_any && h.inside && h.exit > h.z) {
+    h = h0;
+    hit_any = false;
+    for (uint32_t i = 0; i < S.n_objects; i++) {
       if (i == skip) continue;
-      if (object_hit<ANY>(S, i, w, h, stack, flags)) {
-        hit_any = true;
-        if (ANY) return true;
-      }
+      if (object_hit<false>(S, i, w, h, stack, flags, kRefOrder)) hit_any = true;
     }
   }
   return hit_any;
