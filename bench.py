@@ -1,0 +1,346 @@
+"""bench.py — throughput of lambda's spectral path-tracing render on B200.
+
+Workload (the instanced configuration): 64 instances of one seeded displaced
+icosphere (subdivision 7, 327,680 triangles) on a 2-triangle ground plane
+under 2 quad lights; materials drawn uniformly from Lambertian / Blinn /
+thin film; 1920x1080, 64 spp, 32 bounces, p = 0.8; the reference's spectral
+constants (16 hero wavelengths on 400-720 nm, 80 bins).  Inputs are seeded
+synthetic scenes (lambda_b200/synth.py) standing in for the reference's
+benchmark scenes, which it does not ship.
+
+A step is one render of the full frame: W*H*spp paths (one path = one
+camera sample carrying 16 hero wavelengths, Renderer::tracePath).
+
+    python bench.py [--gpus N --steps K --warmup W]       # device arm
+    python bench.py --impl reference [...]                # reference CPU arm
+
+value: Mpaths/s of the render kernel with the scene resident on the device
+(CUDA events on the launching stream, L2 flushed between timed steps, max
+over ranks).  e2e: the same metric through the C ABI with host buffers —
+lgpu_upload_scene (host layout + host-to-device copies) plus lgpu_render
+(kernel + device-to-host image) per step.  Multi-GPU: every rank renders
+its own frame (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = ("Mpaths/s at fixed RMSE: plain GPU vs batched vs host CPU; adjoint/forward cost")
+UNIT = "Mpaths/s"
+
+FULL = dict(n_instances=64, subdiv=7, width=1920, spp=64, bounces=32, p=0.8)
+SMALL = dict(n_instances=64, subdiv=7, width=480, spp=2, bounces=32, p=0.8)
+
+# per-unit algorithmic bytes of the traversal (one 8-wide node: 6x8 float
+# bounds + 8 B header; one triangle: 3 float3 vertices; one instance test:
+# M and M_inv; one hit: shading normals + material header)
+BYTES_PER_NODE = 200
+BYTES_PER_TRI = 36
+BYTES_PER_INST = 128
+BYTES_PER_RAY = 64
+
+
+def workload_desc(w):
+    return ("instanced: %d x displaced icosphere (subdivision %d, %d tris), 2-tri ground, "
+            "2 quad lights, %dx%d, %d spp, %d bounces, p=%.1f, 16 hero wavelengths 400-720 nm "
+            "(80 bins)" % (w["n_instances"], w["subdiv"], 20 * 4 ** w["subdiv"], w["width"],
+                           int(round(w["width"] * 9 / 16)), w["spp"], w["bounces"], w["p"]))
+
+
+def make_scene(w, cache=None):
+    from lambda_b200 import synth
+    cache = cache or os.environ.get("LGPU_BENCH_CACHE") or os.path.join(tempfile.gettempdir(),
+                                                                       "lgpu_bench")
+    d = os.path.join(cache, "instanced_%d_%d_%d" % (w["n_instances"], w["subdiv"], w["width"]))
+    nls = os.path.join(d, "scene.nls")
+    if not os.path.exists(nls):
+        synth.instanced(d, n_instances=w["n_instances"], subdiv=w["subdiv"], width=w["width"])
+    return nls
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profile_traffic_per_path():
+    """DRAM bytes per path of the render kernel from the committed ncu
+    summary (profiles/render_instanced_small.json), or None."""
+    p = os.path.join(REPO, "profiles", "render_instanced_small.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["dram_bytes_per_path"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def cpu_reference_sample(nls, w, budget_s, fast=True):
+    """Times the reference's own pixel loop (oracle/_ref, -O3 OpenMP build)
+    over rows spread across the image; returns (paths/s, cores, sample)."""
+    from oracle import refharness
+    ref = refharness.RefScene(nls, fast=fast)
+    cores = ref.L.ref_max_threads()
+    H = ref.height
+    t0 = time.perf_counter()
+    ref.render_rows(w["spp"], w["bounces"], w["p"], H // 2, H // 2 + 1)
+    one = max(time.perf_counter() - t0, 1e-3)
+    n_rows = int(max(1, min(H, budget_s / one)))
+    rows = sorted(set(int(round(x)) for x in
+                      [i * (H - 1) / max(n_rows - 1, 1) for i in range(n_rows)]))
+    t0 = time.perf_counter()
+    for r in rows:
+        ref.render_rows(w["spp"], w["bounces"], w["p"], r, r + 1)
+    dt = time.perf_counter() - t0
+    paths = len(rows) * ref.width * w["spp"]
+    sample = "%d of %d rows (evenly spread) x %d px x %d spp = %d paths" % (
+        len(rows), H, ref.width, w["spp"], paths)
+    return paths / dt, cores, sample
+
+
+def run_reference(args, w):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import refharness
+    if not refharness.available(fast=True):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/libref_fast.so was not built"}))
+        return 0
+    nls = make_scene(w)
+    for _ in range(args.warmup):
+        cpu_reference_sample(nls, w, args.ref_step_s)
+    vals, cores, sample = [], 0, ""
+    for _ in range(args.steps):
+        v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
+        vals.append(v)
+    value = statistics.mean(vals) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": workload_desc(w), "cpu": "reference Renderer pixel loop, "
+                       "-O3 -fopenmp -march=x86-64-v3 build of the reference sources"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def run_device(args, w):
+    import torch
+
+    from lambda_b200.renderer import Context
+    from lambda_b200.scene import flatten, load_nls
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+
+    nls = make_scene(w)
+    sc = load_nls(nls)
+    fs = flatten(sc)
+    ctx = Context(local)
+    ctx.upload(fs)
+    W, H = ctx.size
+    spp, B, p = w["spp"], w["bounces"], w["p"]
+    paths_per_step = W * H * spp
+    d_out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    stream = torch.cuda.current_stream()
+
+    def step(seed):
+        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=seed, stream=stream.cuda_stream)
+
+    for k in range(args.warmup):
+        step(1000 + k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    step_ms, kern_ms, counters = [], [], []
+    for k in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step(k)
+        e1.record(stream)
+        e1.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        st = ctx.stats()
+        kern_ms.append(st["last_kernel_ms"])
+        counters.append(st)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    total_ms = sum(step_ms)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * paths_per_step * args.steps / (total_ms / 1e3) / 1e6
+
+    # end to end through the C ABI with host buffers
+    import numpy as np
+    host = np.empty((H, W, 3), np.float32)
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        ctx.upload(fs)
+        ctx.render(spp, B, p, seed=k, out=host)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = ctx.stats()["upload_bytes"]
+    e2e = {"value": world * paths_per_step * e2e_steps / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(W * H * 3 * 4),
+           "note": "lgpu_upload_scene (host layout + copies) + lgpu_render (kernel + image "
+                   "readback) per step"}
+
+    c = counters[-1]
+    algo = (c["node_tests"] * BYTES_PER_NODE + c["tri_tests"] * BYTES_PER_TRI +
+            c["inst_tests"] * BYTES_PER_INST + c["rays"] * BYTES_PER_RAY)
+    avg_kernel_s = statistics.mean(kern_ms) / 1e3
+    peak, peak_kind = measured_peak_hbm()
+    achieved = algo / avg_kernel_s / 1e9
+    tpp = profile_traffic_per_path()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": (tpp * paths_per_step) if tpp is not None else None,
+                "algorithmic_bytes_per_launch": int(algo),
+                "per_launch": {"paths": int(c["paths"]), "rays": int(c["rays"]),
+                               "node_tests": int(c["node_tests"]), "tri_tests": int(c["tri_tests"]),
+                               "inst_tests": int(c["inst_tests"])},
+                "mrays_per_s": c["rays"] / avg_kernel_s / 1e6}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded scene generator)",
+            "config": {"workload": workload_desc(w), "paths_per_step_per_gpu": paths_per_step,
+                       "l2": "256 MB buffer written between timed steps",
+                       "parallelism": "frame per GPU" if world > 1 else "single GPU"},
+            "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps,
+            "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
+    if rank == 0 and world == 1 and not args.no_baseline:
+        from oracle import refharness
+        if refharness.available(fast=True):
+            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
+            line["cpu_baseline"] = {"value": v / 1e6, "unit": UNIT, "cores": cores,
+                                    "kind": "reference", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lgpu", choices=["lgpu", "reference"])
+    ap.add_argument("--small", action="store_true", help="reduced frame (profiling)")
+    ap.add_argument("--spp", type=int, default=None)
+    ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--ref-step-s", type=float, default=8.0,
+                    help="seconds of reference CPU work per sampled step")
+    args = ap.parse_args()
+    w = dict(SMALL if args.small else FULL)
+    if args.spp:
+        w["spp"] = args.spp
+    if args.impl == "reference":
+        return run_reference(args, w)
+    return run_device(args, w)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -215,6 +215,10 @@ typedef struct lgpu_stats {
   uint32_t max_stack;       /* traversal stack bound in use */
   uint32_t nonfinite_paths; /* paths whose radiance was NaN or infinite */
   uint32_t reserved;
+  uint64_t node_tests; /* 8-wide node box tests of the last kernel */
+  uint64_t tri_tests;  /* triangle tests */
+  uint64_t inst_tests; /* object (instance) tests */
+  uint64_t upload_bytes; /* host-to-device bytes of the last scene upload */
 } lgpu_stats;
 
 /* Context.  `device` is a CUDA ordinal. */

@@ -121,6 +121,9 @@ int collect(lgpu_ctx* ctx, const char* what) {
   ctx->stats.rays = c.rays;
   ctx->stats.paths = c.paths;
   ctx->stats.device_checks = c.flags;
+  ctx->stats.node_tests = c.nodes;
+  ctx->stats.tri_tests = c.tris;
+  ctx->stats.inst_tests = c.insts;
   ctx->stats.nonfinite_paths = c.nonfinite;
   if (c.flags & 1u)
     return fail(ctx, LGPU_ERR_DEVICE_CHECK,
@@ -252,6 +255,12 @@ int lgpu_upload_scene(lgpu_ctx* ctx, const lgpu_scene* scene) {
   S.cam = scene->cam;
   std::memcpy(S.tlas_bounds, L.tlas_bounds, sizeof(S.tlas_bounds));
   ctx->stats.max_stack = L.max_stack;
+  ctx->stats.upload_bytes =
+      L.objects.size() * sizeof(DevObject) + L.meshes.size() * sizeof(DevMesh) +
+      L.nodes.size() * sizeof(WideNode) + L.tris.size() * sizeof(TriSlot) +
+      L.shade.size() * sizeof(FaceShade) + L.spectra.size() * sizeof(float) +
+      L.mats.size() * sizeof(DevMaterial) + L.lights.size() * sizeof(lgpu_light) +
+      L.tlas_objects.size() * sizeof(uint32_t) + L.cmf.size() * sizeof(float);
   ctx->has_scene = true;
   return LGPU_OK;
 }

@@ -207,6 +207,15 @@ struct StackEntry {
   float t;
 };
 
+// Per-thread traversal counters: flags (bit 0: a stack bound was hit) and
+// the work done, for the roofline's algorithmic byte count.
+struct TravStats {
+  uint32_t flags;
+  uint32_t nodes;  // wide nodes whose 8 child boxes were tested
+  uint32_t tris;   // triangle tests
+  uint32_t insts;  // object (instance) tests
+};
+
 // Tests the children of an interior node and pushes the hit ones so that
 // the nearest is on top; equal distances keep child order, as the
 // reference's insertion-sorted std::sort of <= 8 elements does
@@ -325,7 +334,7 @@ enum Order { kRefOrder = 0, kTlasClosest = 1, kTlasAny = 2 };
 template <bool ANY>
 __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, const DevObject& ob,
                                             const Ray& w, HitRec& h, StackEntry* stack,
-                                            uint32_t& flags, int order) {
+                                            TravStats& ts, int order) {
   Ray const l = to_local(ob, w);
   const DevMesh& m = S.meshes[ob.mesh];
   bool inside;
@@ -342,8 +351,9 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
     if (e.t > h.z) continue;
     if (!(e.ref & kLeafBit)) {
       const WideNode& nd = S.nodes[e.ref];
+      ts.nodes++;
       if (!push_children(nd, l, h.z, stack, sp, kStackCap)) {
-        flags |= 1u;
+        ts.flags |= 1u;
         break;
       }
       continue;
@@ -352,6 +362,7 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
     uint32_t const slot = e.ref & kSlotMask;
     for (uint32_t k = 0; k < count; k++) {
       const TriSlot& T = S.tris[slot + k];
+      ts.tris++;
       float t, b0, b1, b2;
       if (tri_test(T, l, mr, h.z, t, b0, b1, b2)) {
         h.z = t;
@@ -373,9 +384,10 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
 
 template <bool ANY>
 __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const Ray& w, HitRec& h,
-                                           StackEntry* stack, uint32_t& flags, int order) {
+                                           StackEntry* stack, TravStats& ts, int order) {
   const DevObject& ob = S.objects[i];
-  if (ob.type == LGPU_OBJ_TRIMESH) return trimesh_hit<ANY>(S, i, ob, w, h, stack, flags, order);
+  ts.insts++;
+  if (ob.type == LGPU_OBJ_TRIMESH) return trimesh_hit<ANY>(S, i, ob, w, h, stack, ts, order);
   Ray const l = to_local(ob, w);
   float t;
   if (ob.type == LGPU_OBJ_SPHERE) {
@@ -411,13 +423,13 @@ __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const 
 template <bool ANY>
 __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRec& h, uint32_t skip,
                                           bool reference_order, StackEntry* stack,
-                                          StackEntry* tstack, uint32_t& flags) {
+                                          StackEntry* tstack, TravStats& ts) {
   h.inside = false;
   if (reference_order || S.n_objects <= 4) {
     bool hit_any = false;
     for (uint32_t i = 0; i < S.n_objects; i++) {
       if (i == skip) continue;
-      if (object_hit<ANY>(S, i, w, h, stack, flags, kRefOrder)) {
+      if (object_hit<ANY>(S, i, w, h, stack, ts, kRefOrder)) {
         hit_any = true;
         if (ANY) return true;
       }
@@ -435,8 +447,9 @@ __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRe
       StackEntry const e = tstack[--sp];
       if (e.t > h.z) continue;
       if (!(e.ref & kLeafBit)) {
+        ts.nodes++;
         if (!push_children(S.nodes[e.ref], w, h.z, tstack, sp, kTlasStackCap)) {
-          flags |= 1u;
+          ts.flags |= 1u;
           break;
         }
         continue;
@@ -447,7 +460,7 @@ __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRe
         uint32_t const i = S.tlas_objects[slot + k];
         if (i == skip) continue;
         if (ANY) {
-          if (object_hit<true>(S, i, w, h, stack, flags, order)) return true;
+          if (object_hit<true>(S, i, w, h, stack, ts, order)) return true;
           continue;
         }
         // a lower-index object loses ties: test it against the next float
@@ -455,7 +468,7 @@ __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRe
         float const zs = h.z;
         bool const lowered = (h.obj != UINT32_MAX && i < h.obj);
         if (lowered) h.z = prev_float(zs);
-        if (object_hit<false>(S, i, w, h, stack, flags, order)) hit_any = true;
+        if (object_hit<false>(S, i, w, h, stack, ts, order)) hit_any = true;
         else if (lowered) h.z = zs;
       }
     }
@@ -465,7 +478,7 @@ __device__ __forceinline__ bool scene_hit(const DevScene& S, const Ray& w, HitRe
     hit_any = false;
     for (uint32_t i = 0; i < S.n_objects; i++) {
       if (i == skip) continue;
-      if (object_hit<false>(S, i, w, h, stack, flags, kRefOrder)) hit_any = true;
+      if (object_hit<false>(S, i, w, h, stack, ts, kRefOrder)) hit_any = true;
     }
   }
   return hit_any;

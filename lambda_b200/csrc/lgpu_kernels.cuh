@@ -11,8 +11,11 @@ namespace lgpu {
 struct DevCounters {
   unsigned long long rays;
   unsigned long long paths;
-  unsigned int flags;     // bit 0: traversal stack overflow
-  unsigned int nonfinite; // paths whose radiance was NaN or infinite
+  unsigned long long nodes;  // wide-node child-box tests
+  unsigned long long tris;   // triangle tests
+  unsigned long long insts;  // object tests
+  unsigned int flags;        // bit 0: traversal stack overflow
+  unsigned int nonfinite;    // paths whose radiance was NaN or infinite
 };
 
 struct RenderArgs {
@@ -32,6 +35,9 @@ cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uin
 
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
                           cudaStream_t st);
+template <int K>
+cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
+                            cudaStream_t st);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
 // doubles, at least tonemap_partials_needed(n)).

@@ -150,11 +150,11 @@ struct LightSample {
 };
 
 __device__ __forceinline__ bool occluded(const DevScene& S, f3 p, f3 d, float tmax, uint32_t skip,
-                                         bool ref_order, Stacks& st, uint32_t& flags) {
+                                         bool ref_order, Stacks& st, TravStats& ts) {
   HitRec h;
   h.z = tmax;
   h.obj = UINT32_MAX;
-  return scene_hit<true>(S, make_ray(p, d), h, skip, ref_order, st.mesh, st.tlas, flags);
+  return scene_hit<true>(S, make_ray(p, d), h, skip, ref_order, st.mesh, st.tlas, ts);
 }
 
 __device__ __forceinline__ f3 col3(const float* M16, int c) {
@@ -164,7 +164,7 @@ __device__ __forceinline__ f3 col3(const float* M16, int c) {
 // sample::light (cg.hpp:1560-1732) including the shadow ray
 __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgpu_light& L,
                                                     const HitInfo& H, uint64_t& rng, bool ref_order,
-                                                    Stacks& st, uint32_t& flags, uint32_t& rays) {
+                                                    Stacks& st, TravStats& ts, uint32_t& rays) {
   LightSample ls;
   ls.scale = 0.f;
   ls.prob = 1.f;
@@ -188,7 +188,7 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
                   B.x.y * stt * cp + B.y.y * stt * sp + B.z.y * ct,
                   B.x.z * stt * cp + B.y.z * stt * sp + B.z.z * ct};
       rays++;
-      ls.scale = occluded(S, H.p, ls.dir, sqrtf(dist2), L.obj, ref_order, st, flags) ? 0.f : 1.f;
+      ls.scale = occluded(S, H.p, ls.dir, sqrtf(dist2), L.obj, ref_order, st, ts) ? 0.f : 1.f;
       break;
     }
     case LGPU_LIGHT_QUADDIR: {  // cg.hpp:1625-1655
@@ -206,7 +206,7 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
       float const pr = (L.spec + 1.f) * 0.5f * kInvPi * cos_spec * L.inv_area;
       ls.prob = 1e-6f >= pr ? 1e-6f : pr;
       rays++;
-      bool const occ = occluded(S, H.p, w, sqrtf(dist2), L.obj, ref_order, st, flags);
+      bool const occ = occluded(S, H.p, w, sqrtf(dist2), L.obj, ref_order, st, ts);
       ls.scale = occ ? 0.f : cos_spec;
       break;
     }
@@ -215,14 +215,14 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
       ls.dir = fnorm(Lv);
       float const dist = sqrtf(fdot(Lv, Lv));
       rays++;
-      bool const occ = occluded(S, H.p, ls.dir, dist, UINT32_MAX, ref_order, st, flags);
+      bool const occ = occluded(S, H.p, ls.dir, dist, UINT32_MAX, ref_order, st, ts);
       ls.scale = occ ? 0.f : 1.f / (dist * dist);
       break;
     }
     case LGPU_LIGHT_DIR: {  // cg.hpp:1604-1621
       ls.dir = f3{-L.dir[0], -L.dir[1], -L.dir[2]};
       rays++;
-      ls.scale = occluded(S, H.p, ls.dir, kFltMax, UINT32_MAX, ref_order, st, flags) ? 0.f : 1.f;
+      ls.scale = occluded(S, H.p, ls.dir, kFltMax, UINT32_MAX, ref_order, st, ts) ? 0.f : 1.f;
       break;
     }
     default: {  // ambient, cg.hpp:1560-1577
@@ -565,7 +565,7 @@ __device__ __forceinline__ float prob_for_material(const DevScene& S, const DevM
 
 struct PathCounters {
   uint32_t rays;
-  uint32_t flags;
+  TravStats ts;
 };
 
 // Renderer::tracePath (src/renderer.cpp:64-146) for the camera ray r with
@@ -589,7 +589,7 @@ __device__ __forceinline__ void trace_path(const DevScene& S, Ray r, float hero,
     h.z = kFltMax;
     h.obj = UINT32_MAX;
     pc.rays++;
-    if (!scene_hit<false>(S, r, h, UINT32_MAX, ref_order, st.mesh, st.tlas, pc.flags)) return;
+    if (!scene_hit<false>(S, r, h, UINT32_MAX, ref_order, st.mesh, st.tlas, pc.ts)) return;
     HitInfo const H = finalize_hit(S, r, h);
     f3 const un = fnorm(r.u);
     f3 const o = f3{-un.x, -un.y, -un.z};
@@ -611,7 +611,7 @@ __device__ __forceinline__ void trace_path(const DevScene& S, Ray r, float hero,
     uint32_t const li = (uint32_t)(lgpu_u64(&rng) % (uint64_t)S.n_lights);
     float const prob_l = 1.f / (float)S.n_lights;
     const lgpu_light& L = S.lights[li];
-    LightSample const ls = sample_light(S, L, H, rng, ref_order, st, pc.flags, pc.rays);
+    LightSample const ls = sample_light(S, L, H, rng, ref_order, st, pc.ts, pc.rays);
     BsdfScalars const bl = bsdf_scalars(S, m, xk[0], ls.dir, o, n, H.front);
 
     // material importance sample (src/renderer.cpp:109-120)

@@ -1,0 +1,94 @@
+// lgpu_render.cuh — the render kernel, instantiated per hero-wavelength
+// count in lgpu_render_k{4,8,16}.cu (separate units compile in parallel).
+#pragma once
+
+#include "lgpu_counters.cuh"
+#include "lgpu_path.cuh"
+
+namespace lgpu {
+
+// Renderer::render (src/renderer.cpp:14-61) for a range of pixels: one
+// thread per pixel, all of its samples, film accumulated as XYZ.
+template <int K>
+__global__ void __launch_bounds__(128) render_kernel(DevScene S, RenderArgs a, float* __restrict__ out,
+                                                     DevCounters* cnt) {
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t rays = 0, nonfinite = 0, paths = 0;
+  TravStats ts{0u, 0u, 0u, 0u};
+  if (t < a.pixel_count) {
+    uint32_t const pix = a.pixel_begin + t;
+    uint32_t const W = uint32_t(S.cam.width), H = uint32_t(S.cam.height);
+    uint32_t const i = pix / W, j = pix - i * W;
+    float const omega = S.lambda_sup - S.lambda_inf;
+    float const step = omega / float(K);
+    float const prob_l = 1.f / omega;
+    bool const ref_order = (a.flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
+    const lgpu_camera& C = S.cam;
+    f3 const Fx = f3{C.base_x[0], C.base_x[1], C.base_x[2]};
+    f3 const Fy = f3{C.base_y[0], C.base_y[1], C.base_y[2]};
+    f3 const Fz = f3{C.base_z[0], C.base_z[1], C.base_z[2]};
+    f3 const P = f3{C.pos[0], C.pos[1], C.pos[2]};
+    Stacks st;
+    float X = 0.f, Y = 0.f, Z = 0.f;
+    uint64_t const stream = (uint64_t(a.stream_tag) << 32) | pix;
+    for (uint32_t s = 0; s < a.spp; s++) {
+      uint64_t rng = lgpu_path_state(a.seed, stream, uint64_t(a.spp_offset) + s);
+      float const u = float(j) + lgpu_flt(&rng);
+      float const v = float(i) + lgpu_flt(&rng);
+      // sample::camera (cg.hpp:1534-1542)
+      float const cu = -0.5f * C.w + C.delta * u;
+      float const cv = -0.5f * C.h + C.delta * v;
+      f3 const wij = f3{P.x + Fx.x * cu + Fy.x * cv - C.D * Fz.x, P.y + Fx.y * cu + Fy.y * cv - C.D * Fz.y,
+                        P.z + Fx.z * cu + Fy.z * cv - C.D * Fz.z};
+      float const la = lgpu_flt(&rng) - 0.5f;
+      float const lb = lgpu_flt(&rng) - 0.5f;
+      float const dd = 2.f * C.dof;
+      f3 const wkl = f3{P.x + dd * (Fx.x * la + Fy.x * lb), P.y + dd * (Fx.y * la + Fy.y * lb),
+                        P.z + dd * (Fx.z * la + Fy.z * lb)};
+      f3 const dir = fnorm(f3{wij.x - wkl.x, wij.y - wkl.y, wij.z - wkl.z});
+      // sample::spectrum (cg.hpp:1517-1531)
+      float const hero = S.lambda_inf + omega * lgpu_flt(&rng);
+      float acc[K];
+      PathCounters pc{0u, ts};
+      trace_path<K>(S, make_ray(wkl, dir), hero, step, a.max_scatter, a.sample_p, ref_order, rng, acc, st,
+                    pc);
+      rays += pc.rays;
+      ts = pc.ts;
+      paths++;
+      // addHeroλ(λ, Li/prob) (src/renderer.cpp:44)
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      bool finite = true;
+#pragma unroll
+      for (int k = 0; k < K; k++) {
+        float const val = acc[k] / prob_l;
+        finite = finite && isfinite(val);
+        splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
+      }
+      nonfinite += finite ? 0u : 1u;
+      X += sx;
+      Y += sy;
+      Z += sz;
+    }
+    // irradiance / (SPP*K), dotted with the CMFs times Δ, then XYZ2linRGB
+    // (src/renderer.cpp:52-56, cg.hpp:144-148, 340-341)
+    float const norm = float(a.spp * K);
+    X = (X / norm) * S.lambda_delta;
+    Y = (Y / norm) * S.lambda_delta;
+    Z = (Z / norm) * S.lambda_delta;
+    size_t const o = (size_t(H - i - 1) * W + j) * 3;
+    out[o + 0] = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
+    out[o + 1] = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
+    out[o + 2] = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
+  }
+  flush_counters(cnt, rays, paths, ts, nonfinite);
+}
+
+template <int K>
+cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
+                            cudaStream_t st) {
+  uint32_t const blocks = (a.pixel_count + 127) / 128;
+  render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
+  return cudaGetLastError();
+}
+
+}  // namespace lgpu

@@ -107,7 +107,9 @@ class Context:
         L.check(self.h, self._lib.lgpu_get_stats(self.h, ctypes.byref(s)), "stats")
         return {"last_kernel_ms": s.last_kernel_ms, "rays": s.rays, "paths": s.paths,
                 "device_checks": s.device_checks, "max_stack": s.max_stack,
-                "nonfinite_paths": s.nonfinite_paths}
+                "nonfinite_paths": s.nonfinite_paths, "node_tests": s.node_tests,
+                "tri_tests": s.tri_tests, "inst_tests": s.inst_tests,
+                "upload_bytes": s.upload_bytes}
 
 
 def hits_to_numpy(arr, n):
