@@ -184,6 +184,11 @@ typedef struct lgpu_scene {
    instance-level BVH. */
 #define LGPU_FLAG_REFERENCE_ORDER 0x1u
 
+/* Render with one thread per pixel looping over its samples and bounces
+   (the megakernel) instead of the default wavefront kernels.  Both draw
+   the same random numbers per path. */
+#define LGPU_FLAG_MEGAKERNEL 0x2u
+
 /* Renderer settings (include/renderer.hpp:35-37) plus the device RNG seed. */
 typedef struct lgpu_render_params {
   uint32_t spp;             /* Renderer::SPP */

@@ -30,6 +30,7 @@ MAT_LAMBERTIAN, MAT_BLINN, MAT_THINFILM, MAT_MICROFACET, MAT_EMITTER, MAT_DIREMI
 LIGHT_AMBIENT, LIGHT_POINT, LIGHT_DIR, LIGHT_SPHERE, LIGHT_QUADDIR = range(5)
 
 FLAG_REFERENCE_ORDER = 0x1
+FLAG_MEGAKERNEL = 0x2
 
 
 class Transform(ctypes.Structure):

@@ -48,6 +48,11 @@ struct lgpu_ctx {
   DevArray<float> cmf;
   // working buffers
   DevArray<float> out;
+  // wavefront state (lgpu_wave.cuh), sized for the last frame rendered
+  DevArray<float> w_ray, w_hero, w_beta, w_acc, w_hit, w_sray, w_scontrib, w_film;
+  DevArray<uint64_t> w_rng;
+  DevArray<uint32_t> w_depth, w_q0, w_q1, w_spath, w_counts;
+  uint32_t w_cap = 0, w_k = 0, w_npix = 0;
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
   DevArray<double> partials;
@@ -131,6 +136,57 @@ int collect(lgpu_ctx* ctx, const char* what) {
   return LGPU_OK;
 }
 
+// Sizes the wavefront buffers for a frame of npix pixels and fills ws.
+int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
+  uint32_t const K = ctx->S.hero_k;
+  uint32_t const ns = wave_samples(npix, spp);
+  uint32_t const cap = npix * ns;
+  if (cap != ctx->w_cap || K != ctx->w_k || npix != ctx->w_npix) {
+    size_t const c = cap;
+    cudaError_t e = ensure(ctx->w_ray, 6 * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_hero, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_beta, size_t(K) * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_acc, size_t(K) * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_hit, 9 * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_sray, 8 * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_scontrib, size_t(K) * c);
+    if (e == cudaSuccess) e = ensure(ctx->w_film, 3 * size_t(npix));
+    if (e == cudaSuccess) e = ensure(ctx->w_rng, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_depth, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_q0, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_q1, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_spath, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_counts, 4);
+    if (e != cudaSuccess) {
+      ctx->w_cap = 0;
+      return cuda_fail(ctx, e, "wavefront buffers");
+    }
+    ctx->w_cap = cap;
+    ctx->w_k = K;
+    ctx->w_npix = npix;
+  }
+  ws.cap = cap;
+  ws.npix = npix;
+  ws.n_samples = ns;
+  ws.ray = ctx->w_ray.ptr;
+  ws.rng = ctx->w_rng.ptr;
+  ws.hero = ctx->w_hero.ptr;
+  ws.depth = ctx->w_depth.ptr;
+  ws.beta = ctx->w_beta.ptr;
+  ws.acc = ctx->w_acc.ptr;
+  ws.hit = ctx->w_hit.ptr;
+  ws.q_in = ctx->w_q0.ptr;
+  ws.q_out = ctx->w_q1.ptr;
+  ws.n_in = ctx->w_counts.ptr;
+  ws.n_out = ctx->w_counts.ptr + 1;
+  ws.n_shadow = ctx->w_counts.ptr + 2;
+  ws.sray = ctx->w_sray.ptr;
+  ws.s_path = ctx->w_spath.ptr;
+  ws.s_contrib = ctx->w_scontrib.ptr;
+  ws.film = ctx->w_film.ptr;
+  return LGPU_OK;
+}
+
 int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaStream_t st) {
   if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
   if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
@@ -143,9 +199,16 @@ int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaSt
   a.spp_offset = p->spp_offset;
   a.pixel_begin = 0;
   a.pixel_count = uint32_t(ctx->S.cam.width * ctx->S.cam.height);
+  WaveState ws{};
+  WaveState* wave = nullptr;
+  if (!(p->flags & LGPU_FLAG_MEGAKERNEL)) {
+    int const r = ensure_wave(ctx, a.pixel_count, a.spp, ws);
+    if (r != LGPU_OK) return r;
+    wave = &ws;
+  }
   cudaError_t e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  if (e == cudaSuccess) e = launch_render(ctx->S, a, d_out, ctx->counters, st);
+  if (e == cudaSuccess) e = launch_render(ctx->S, a, wave, d_out, ctx->counters, st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return LGPU_OK;
@@ -186,6 +249,12 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->release_scene();
   ctx->out.release();
+  for (DevArray<float>* a : {&ctx->w_ray, &ctx->w_hero, &ctx->w_beta, &ctx->w_acc, &ctx->w_hit,
+                             &ctx->w_sray, &ctx->w_scontrib, &ctx->w_film})
+    a->release();
+  ctx->w_rng.release();
+  for (DevArray<uint32_t>* a : {&ctx->w_depth, &ctx->w_q0, &ctx->w_q1, &ctx->w_spath, &ctx->w_counts})
+    a->release();
   ctx->rays.release();
   ctx->hits.release();
   ctx->partials.release();

@@ -18,6 +18,30 @@ struct DevCounters {
   unsigned int nonfinite;    // paths whose radiance was NaN or infinite
 };
 
+// Device buffers of the wavefront renderer (lgpu_wave.cuh), per-path state
+// in structure-of-arrays layout; the context owns them.
+struct WaveState {
+  uint32_t cap;      // path slots
+  uint32_t npix;     // pixels of the frame
+  uint32_t n_samples;  // samples per pixel in this wave (cap >= npix*n_samples)
+  float* ray;        // 6*cap (ox, oy, oz, dx, dy, dz), field-major
+  uint64_t* rng;     // cap
+  float* hero;       // cap
+  uint32_t* depth;   // cap
+  float* beta;       // K*cap
+  float* acc;        // K*cap
+  float* hit;        // 9*cap (z, obj, face, b0, b1, b2, plx, ply, plz)
+  uint32_t* q_in;    // active path slots
+  uint32_t* q_out;
+  uint32_t* n_in;    // device counts
+  uint32_t* n_out;
+  float* sray;       // 8*cap (ox, oy, oz, dx, dy, dz, tmax, skip)
+  uint32_t* s_path;  // cap
+  float* s_contrib;  // K*cap
+  uint32_t* n_shadow;
+  float* film;       // 3*npix XYZ
+};
+
 struct RenderArgs {
   uint32_t spp;
   uint32_t max_scatter;
@@ -33,11 +57,23 @@ struct RenderArgs {
 cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
                          lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st);
 
-cudaError_t launch_render(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
-                          cudaStream_t st);
+cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
+                          DevCounters* d_cnt, cudaStream_t st);
+// Renders with the wavefront kernels when wave != nullptr, else with the
+// one-thread-per-pixel megakernel.
 template <int K>
-cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
-                            cudaStream_t st);
+cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
+                            DevCounters* d_cnt, cudaStream_t st);
+
+// Samples per pixel in one wave for a frame of npix pixels: enough paths in
+// flight to fill the GPU (about 2^21), never more than spp.
+uint32_t wave_samples(uint32_t npix, uint32_t spp);
+
+// XYZ film (3 floats per pixel, scene row order) / norm * delta ->
+// linear BT.709 RGB in the reference's layout (row 0 at the top),
+// src/renderer.cpp:52-56.
+cudaError_t launch_finalize(const float* film, uint32_t npix, uint32_t W, uint32_t H, float norm,
+                            float delta, float* out, cudaStream_t st);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
 // doubles, at least tonemap_partials_needed(n)).

@@ -161,14 +161,19 @@ __device__ __forceinline__ f3 col3(const float* M16, int c) {
   return f3{M16[c], M16[4 + c], M16[8 + c]};
 }
 
-// sample::light (cg.hpp:1560-1732) including the shadow ray
-__device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgpu_light& L,
-                                                    const HitInfo& H, uint64_t& rng, bool ref_order,
-                                                    Stacks& st, TravStats& ts, uint32_t& rays) {
+// sample::light (cg.hpp:1560-1732) without its shadow ray: `scale` is the
+// λ-independent factor of mult assuming the light is visible; tmax and skip
+// describe the shadow ray the reference traces (for sphere lights up to the
+// light's centre, cg.hpp:1696); tmax < 0 means no shadow ray (ambient).
+__device__ __forceinline__ LightSample sample_light_unoccluded(const DevScene& S, const lgpu_light& L,
+                                                               const HitInfo& H, uint64_t& rng,
+                                                               float& tmax, uint32_t& skip) {
   LightSample ls;
   ls.scale = 0.f;
   ls.prob = 1.f;
   ls.dir = f3{0.f, 0.f, 1.f};
+  tmax = -1.f;
+  skip = UINT32_MAX;
   switch (L.type) {
     case LGPU_LIGHT_SPHERE: {  // cg.hpp:1671-1699
       f3 const pos = col3(L.T.M, 3);
@@ -187,8 +192,9 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
       ls.dir = f3{B.x.x * stt * cp + B.y.x * stt * sp + B.z.x * ct,
                   B.x.y * stt * cp + B.y.y * stt * sp + B.z.y * ct,
                   B.x.z * stt * cp + B.y.z * stt * sp + B.z.z * ct};
-      rays++;
-      ls.scale = occluded(S, H.p, ls.dir, sqrtf(dist2), L.obj, ref_order, st, ts) ? 0.f : 1.f;
+      tmax = sqrtf(dist2);
+      skip = L.obj;
+      ls.scale = 1.f;
       break;
     }
     case LGPU_LIGHT_QUADDIR: {  // cg.hpp:1625-1655
@@ -205,24 +211,23 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
       float const cos_spec = powf(-fdot(w, nl), L.spec);
       float const pr = (L.spec + 1.f) * 0.5f * kInvPi * cos_spec * L.inv_area;
       ls.prob = 1e-6f >= pr ? 1e-6f : pr;
-      rays++;
-      bool const occ = occluded(S, H.p, w, sqrtf(dist2), L.obj, ref_order, st, ts);
-      ls.scale = occ ? 0.f : cos_spec;
+      tmax = sqrtf(dist2);
+      skip = L.obj;
+      ls.scale = cos_spec;
       break;
     }
     case LGPU_LIGHT_POINT: {  // cg.hpp:1580-1601
       f3 const Lv = f3{L.pos[0] - H.p.x, L.pos[1] - H.p.y, L.pos[2] - H.p.z};
       ls.dir = fnorm(Lv);
       float const dist = sqrtf(fdot(Lv, Lv));
-      rays++;
-      bool const occ = occluded(S, H.p, ls.dir, dist, UINT32_MAX, ref_order, st, ts);
-      ls.scale = occ ? 0.f : 1.f / (dist * dist);
+      tmax = dist;
+      ls.scale = 1.f / (dist * dist);
       break;
     }
     case LGPU_LIGHT_DIR: {  // cg.hpp:1604-1621
       ls.dir = f3{-L.dir[0], -L.dir[1], -L.dir[2]};
-      rays++;
-      ls.scale = occluded(S, H.p, ls.dir, kFltMax, UINT32_MAX, ref_order, st, ts) ? 0.f : 1.f;
+      tmax = kFltMax;
+      ls.scale = 1.f;
       break;
     }
     default: {  // ambient, cg.hpp:1560-1577
@@ -235,6 +240,20 @@ __device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgp
       ls.scale = 1.f;
       break;
     }
+  }
+  return ls;
+}
+
+// sample::light (cg.hpp:1560-1732) including the shadow ray
+__device__ __forceinline__ LightSample sample_light(const DevScene& S, const lgpu_light& L,
+                                                    const HitInfo& H, uint64_t& rng, bool ref_order,
+                                                    Stacks& st, TravStats& ts, uint32_t& rays) {
+  float tmax;
+  uint32_t skip;
+  LightSample ls = sample_light_unoccluded(S, L, H, rng, tmax, skip);
+  if (tmax >= 0.f) {
+    rays++;
+    if (occluded(S, H.p, ls.dir, tmax, skip, ref_order, st, ts)) ls.scale = 0.f;
   }
   return ls;
 }

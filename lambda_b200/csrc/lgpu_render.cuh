@@ -4,6 +4,7 @@
 
 #include "lgpu_counters.cuh"
 #include "lgpu_path.cuh"
+#include "lgpu_wave.cuh"
 
 namespace lgpu {
 
@@ -83,12 +84,62 @@ __global__ void __launch_bounds__(128) render_kernel(DevScene S, RenderArgs a, f
   flush_counters(cnt, rays, paths, ts, nonfinite);
 }
 
+// Persistent grid size: every SM filled to its occupancy limit.
+template <class F>
+uint32_t persistent_blocks(F kernel, int threads, size_t smem) {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (per_sm < 1) per_sm = 1;
+  return uint32_t(sms * per_sm);
+}
+
 template <int K>
-cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, float* d_out, DevCounters* d_cnt,
-                            cudaStream_t st) {
-  uint32_t const blocks = (a.pixel_count + 127) / 128;
-  render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
-  return cudaGetLastError();
+cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
+                            DevCounters* d_cnt, cudaStream_t st) {
+  if (!wave) {
+    uint32_t const blocks = (a.pixel_count + 127) / 128;
+    render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
+    return cudaGetLastError();
+  }
+  WaveState w = *wave;
+  size_t const smem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
+  static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0;
+  if (!g_trace) {
+    cudaFuncSetAttribute(wf_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(wf_shadow<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    g_trace = persistent_blocks(wf_trace, 128, smem);
+    g_shadow = persistent_blocks(wf_shadow<K>, 128, smem);
+    g_shade = persistent_blocks(wf_shade<K>, 128, 0);
+    g_gen = persistent_blocks(wf_generate, 256, 0);
+  }
+  cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
+  uint32_t const per_wave = w.n_samples;
+  for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += per_wave) {
+    w.n_samples = (a.spp - s0 < per_wave) ? (a.spp - s0) : per_wave;
+    wf_generate<<<g_gen, 256, 0, st>>>(S, a, w, K, s0, d_cnt);
+    // a path scatters at most max_scatter+1 times: max_scatter+2 segments
+    for (uint32_t b = 0; b < a.max_scatter + 2; b++) {
+      cudaMemsetAsync(w.n_out, 0, sizeof(uint32_t), st);
+      cudaMemsetAsync(w.n_shadow, 0, sizeof(uint32_t), st);
+      wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      wf_shade<K><<<g_shade, 128, 0, st>>>(S, a, w, d_cnt);
+      wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      uint32_t* t = w.q_in;
+      w.q_in = w.q_out;
+      w.q_out = t;
+      t = w.n_in;
+      w.n_in = w.n_out;
+      w.n_out = t;
+    }
+    wf_splat<K><<<(w.npix + 255) / 256, 256, 0, st>>>(S, w, d_cnt);
+    e = cudaGetLastError();
+  }
+  w.n_samples = per_wave;
+  if (e == cudaSuccess) e = launch_finalize(w.film, w.npix, uint32_t(S.cam.width), uint32_t(S.cam.height),
+                                            float(a.spp) * float(K), S.lambda_delta, d_out, st);
+  return e;
 }
 
 }  // namespace lgpu

@@ -1,0 +1,212 @@
+// lgpu_traverse.cuh — the instance-level traversal used by the wavefront
+// kernels: one loop over instance-BVH and mesh-BVH nodes with a single
+// stack, so that all lanes of a warp execute the same "pop, test, push"
+// step whatever level they are at.
+//
+// Entering a mesh pushes a marker and the mesh root; popping the marker
+// returns to world space.  A leaf of the instance BVH is consumed one object
+// at a time (the rest of the leaf is pushed back), which visits objects and
+// mesh nodes in exactly the order of the nested traversal in
+// lgpu_intersect.cuh, so results are identical to it (and therefore to the
+// reference's intersect::scene, see scene_hit).
+//
+// The stack keeps its first kSmemStack entries in shared memory, laid out
+// entry-major (entry k of thread t at k*blockDim.x + t) so a warp's pushes
+// and pops hit distinct banks; deeper entries go to a per-thread local
+// array.
+#pragma once
+
+#include "lgpu_intersect.cuh"
+
+namespace lgpu {
+
+constexpr int kSmemStack = 24;
+constexpr int kLocalStack = kStackCap + kTlasStackCap + 4 - kSmemStack;
+constexpr uint32_t kMarker = 0xFFFFFFFEu;
+
+struct SplitStack {
+  StackEntry* sm;  // this thread's column in shared memory
+  uint32_t stride;
+  StackEntry* lm;  // local overflow
+  int sp;
+  __device__ __forceinline__ StackEntry& at(int k) {
+    return k < kSmemStack ? sm[k * stride] : lm[k - kSmemStack];
+  }
+  __device__ __forceinline__ void push(StackEntry e) { at(sp++) = e; }
+  __device__ __forceinline__ StackEntry pop() { return at(--sp); }
+};
+
+constexpr int kSplitCap = kSmemStack + kLocalStack;
+
+// push_children (lgpu_intersect.cuh) writing through a SplitStack
+__device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ray& r, float t_max,
+                                                    SplitStack& st) {
+  bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
+  float t[8];
+  uint32_t ref[8];
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    ref[c] = nd.child[c];
+    t[c] = (ref[c] != kEmptyChild) ? child_box_t(nd, c, r, nx, ny, nz, t_max) : 0.f;
+  }
+  int hits = 0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) hits += (t[c] != 0.f) ? 1 : 0;
+  if (st.sp + hits > kSplitCap) return false;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    if (t[c] == 0.f) continue;
+    int rank = 0;
+#pragma unroll
+    for (int d = 0; d < 8; d++) {
+      if (d == c || t[d] == 0.f) continue;
+      bool const before = (t[d] > t[c]) || (t[d] == t[c] && d < c);
+      rank += before ? 1 : 0;
+    }
+    st.at(st.sp + rank) = StackEntry{ref[c], t[c]};
+  }
+  st.sp += hits;
+  return true;
+}
+
+// Instance-BVH traversal with the same semantics as scene_hit's instance
+// path (ties to the higher object index, inside-bounds meshes tested in full
+// and flagged in the hit).  Returns whether a hit was accepted.
+template <bool ANY>
+__device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitRec& h, uint32_t skip,
+                                           SplitStack& st, TravStats& ts) {
+  h.inside = false;
+  float const t0 = segment_box_entry(S.tlas_bounds, w, h.z);
+  if (t0 == kFltMax) return false;
+  st.sp = 0;
+  st.push(StackEntry{S.tlas_root, t0});
+  bool in_mesh = false, lowered = false, cur_inside = false, hit_any = false;
+  Ray l = w;
+  f3 mr = f3{0.f, 0.f, 0.f};
+  uint32_t cur = 0;
+  float zs = 0.f, cur_exit = 0.f;
+  while (st.sp > 0) {
+    StackEntry const e = st.pop();
+    if (e.ref == kMarker) {
+      in_mesh = false;
+      if (lowered && h.obj != cur) h.z = zs;
+      lowered = false;
+      continue;
+    }
+    if (e.t > h.z) continue;
+    if (!(e.ref & kLeafBit)) {
+      ts.nodes++;
+      if (!push_children_split(S.nodes[e.ref], in_mesh ? l : w, h.z, st)) {
+        ts.flags |= 1u;
+        break;
+      }
+      continue;
+    }
+    uint32_t const cnt = ((e.ref >> 28) & 7u) + 1u;
+    uint32_t const slot = e.ref & kSlotMask;
+    if (in_mesh) {
+      for (uint32_t k = 0; k < cnt; k++) {
+        const TriSlot& T = S.tris[slot + k];
+        ts.tris++;
+        float t, b0, b1, b2;
+        if (tri_test(T, l, mr, h.z, t, b0, b1, b2)) {
+          h.z = t;
+          h.obj = cur;
+          h.face = __float_as_uint(T.v0[3]);
+          h.b0 = b0;
+          h.b1 = b1;
+          h.b2 = b2;
+          h.pl = ray_at(l, t);
+          h.inside = cur_inside;
+          h.exit = cur_exit;
+          hit_any = true;
+          if (ANY) return true;
+        }
+      }
+      continue;
+    }
+    // instance leaf: the first object now, the rest of the leaf afterwards
+    uint32_t const i = S.tlas_objects[slot];
+    if (cnt > 1) {
+      if (st.sp + 1 > kSplitCap) {
+        ts.flags |= 1u;
+        break;
+      }
+      st.push(StackEntry{kLeafBit | ((cnt - 2u) << 28) | (slot + 1u), e.t});
+    }
+    if (i == skip) continue;
+    ts.insts++;
+    const DevObject& ob = S.objects[i];
+    bool const low = !ANY && h.obj != UINT32_MAX && i < h.obj;
+    float const z_saved = h.z;
+    if (low) h.z = prev_float(z_saved);
+    Ray const li = to_local(ob, w);
+    if (ob.type != LGPU_OBJ_TRIMESH) {
+      float t;
+      f3 x;
+      bool hit;
+      if (ob.type == LGPU_OBJ_SPHERE) {
+        hit = sphere_test(li, h.z, t);
+        if (hit) x = ray_at(li, t);
+      } else {
+        hit = plane_test(li, h.z, t, x);
+      }
+      if (hit) {
+        h.z = t;
+        h.obj = i;
+        h.face = UINT32_MAX;
+        h.pl = x;
+        h.inside = false;
+        hit_any = true;
+        if (ANY) return true;
+      } else if (low) {
+        h.z = z_saved;
+      }
+      continue;
+    }
+    const DevMesh& m = S.meshes[ob.mesh];
+    bool inside;
+    float ex;
+    float r0 = aabb_scalar(m.bounds, li, h.z, inside, ex);
+    if (r0 != kFltMax && !ANY && inside) r0 = kBias;
+    if (r0 == kFltMax || r0 > h.z) {
+      if (low) h.z = z_saved;
+      continue;
+    }
+    if (st.sp + 2 > kSplitCap) {
+      ts.flags |= 1u;
+      break;
+    }
+    l = li;
+    mr = cross3(l.p, l.u);
+    cur = i;
+    cur_inside = inside;
+    cur_exit = ex;
+    zs = z_saved;
+    lowered = low;
+    in_mesh = true;
+    st.push(StackEntry{kMarker, 0.f});
+    st.push(StackEntry{m.root, r0});
+  }
+  return hit_any;
+}
+
+// intersect::scene for the wavefront kernels: the instance BVH through
+// trace_tlas, the reference's linear object loop (nested traversal, local
+// stack) for reference order, tiny scenes and the order-dependent case.
+template <bool ANY>
+__device__ __forceinline__ bool scene_trace(const DevScene& S, const Ray& w, HitRec& h, uint32_t skip,
+                                            bool reference_order, SplitStack& st, StackEntry* lstack,
+                                            StackEntry* ltstack, TravStats& ts) {
+  if (reference_order || S.n_objects <= 4)
+    return scene_hit<ANY>(S, w, h, skip, true, lstack, ltstack, ts);
+  HitRec const h0 = h;
+  bool hit = trace_tlas<ANY>(S, w, h, skip, st, ts);
+  if (!ANY && hit && h.inside && h.exit > h.z) {
+    h = h0;
+    hit = scene_hit<false>(S, w, h, skip, true, lstack, ltstack, ts);
+  }
+  return hit;
+}
+
+}  // namespace lgpu

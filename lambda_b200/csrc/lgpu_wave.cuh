@@ -1,0 +1,324 @@
+// lgpu_wave.cuh — wavefront path tracing.
+//
+// A wave is a set of paths (n_samples samples of every pixel) processed one
+// bounce at a time by short kernels over compacted queues:
+//
+//   wf_generate   camera ray + hero wavelengths of every path of the wave
+//   wf_trace      closest hit of every active path          (queue q_in)
+//   wf_shade<K>   emitters, light sample -> shadow ray, material sample ->
+//                 next ray, throughput update                 (q_in -> q_out,
+//                 shadow queue)
+//   wf_shadow<K>  any-hit test of the shadow rays; adds their radiance
+//   wf_splat<K>   adds every path's radiance to its pixel's XYZ film
+//   wf_finalize   film -> linear RGB in the reference's layout
+//
+// Each path draws its random numbers from its own counter-based stream in
+// the same order as Renderer::tracePath (src/renderer.cpp:64-146), so a
+// path's result does not depend on which kernel or slot processes it.
+// Paths are appended to the output queues with one atomic per warp
+// (ballot + popc).  The per-path state is SoA so a warp's accesses to one
+// field are coalesced.  Spectral state (throughput and radiance per hero
+// wavelength) lives in memory and is streamed one wavelength at a time, so
+// the shading kernel keeps no spectral arrays in registers.
+#pragma once
+
+#include "lgpu_counters.cuh"
+#include "lgpu_path.cuh"
+#include "lgpu_traverse.cuh"
+
+namespace lgpu {
+
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
+  unsigned const mask = __activemask();
+  unsigned const b = __ballot_sync(mask, pred);
+  int const lane = threadIdx.x & 31;
+  int const leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader && b) base = atomicAdd(counter, __popc(b));
+  base = __shfl_sync(mask, base, leader);
+  return base + __popc(b & ((1u << lane) - 1u));
+}
+
+// The non-template kernels get internal linkage: every translation unit
+// that instantiates the renderer carries its own copy.
+namespace {
+
+// ---- generate -------------------------------------------------------------------
+
+__global__ void __launch_bounds__(256) wf_generate(DevScene S, RenderArgs a, WaveState w, uint32_t k_hero,
+                                                   uint32_t sample_base, DevCounters* cnt) {
+  uint32_t const n = w.npix * w.n_samples;
+  uint32_t paths = 0;
+  float const omega = S.lambda_sup - S.lambda_inf;
+  const lgpu_camera& C = S.cam;
+  uint32_t const W = uint32_t(C.width);
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+    uint32_t const s_local = p / w.npix;
+    uint32_t const pix = p - s_local * w.npix;
+    uint32_t const i = pix / W, j = pix - i * W;
+    uint64_t rng = lgpu_path_state(a.seed, (uint64_t(a.stream_tag) << 32) | pix,
+                                   uint64_t(a.spp_offset) + sample_base + s_local);
+    float const u = float(j) + lgpu_flt(&rng);
+    float const v = float(i) + lgpu_flt(&rng);
+    f3 const Fx = f3{C.base_x[0], C.base_x[1], C.base_x[2]};
+    f3 const Fy = f3{C.base_y[0], C.base_y[1], C.base_y[2]};
+    f3 const Fz = f3{C.base_z[0], C.base_z[1], C.base_z[2]};
+    f3 const P = f3{C.pos[0], C.pos[1], C.pos[2]};
+    float const cu = -0.5f * C.w + C.delta * u;
+    float const cv = -0.5f * C.h + C.delta * v;
+    f3 const wij = f3{P.x + Fx.x * cu + Fy.x * cv - C.D * Fz.x, P.y + Fx.y * cu + Fy.y * cv - C.D * Fz.y,
+                      P.z + Fx.z * cu + Fy.z * cv - C.D * Fz.z};
+    float const la = lgpu_flt(&rng) - 0.5f;
+    float const lb = lgpu_flt(&rng) - 0.5f;
+    float const dd = 2.f * C.dof;
+    f3 const wkl = f3{P.x + dd * (Fx.x * la + Fy.x * lb), P.y + dd * (Fx.y * la + Fy.y * lb),
+                      P.z + dd * (Fx.z * la + Fy.z * lb)};
+    f3 const dir = fnorm(f3{wij.x - wkl.x, wij.y - wkl.y, wij.z - wkl.z});
+    float const hero = S.lambda_inf + omega * lgpu_flt(&rng);
+    uint32_t const cap = w.cap;
+    w.ray[0 * cap + p] = wkl.x;
+    w.ray[1 * cap + p] = wkl.y;
+    w.ray[2 * cap + p] = wkl.z;
+    w.ray[3 * cap + p] = dir.x;
+    w.ray[4 * cap + p] = dir.y;
+    w.ray[5 * cap + p] = dir.z;
+    w.rng[p] = rng;
+    w.hero[p] = hero;
+    w.depth[p] = 0;
+    for (uint32_t k = 0; k < k_hero; k++) {
+      w.beta[k * cap + p] = 1.f;
+      w.acc[k * cap + p] = 0.f;
+    }
+    w.q_in[p] = p;
+    paths++;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *w.n_in = n;
+  TravStats const ts{0u, 0u, 0u, 0u};
+  flush_counters(cnt, 0u, paths, ts, 0u);
+}
+
+// ---- trace ------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
+  extern __shared__ StackEntry smem_stack[];
+  StackEntry lm[kLocalStack];
+  StackEntry lstack[kStackCap];
+  StackEntry ltstack[kTlasStackCap];
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  TravStats ts{0u, 0u, 0u, 0u};
+  uint32_t rays = 0;
+  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
+  uint32_t const n = *w.n_in;
+  uint32_t const cap = w.cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t const p = w.q_in[i];
+    Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
+                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+    HitRec h;
+    h.z = kFltMax;
+    h.obj = UINT32_MAX;
+    h.face = UINT32_MAX;
+    h.b0 = h.b1 = h.b2 = 0.f;
+    h.pl = f3{0.f, 0.f, 0.f};
+    scene_trace<false>(S, r, h, UINT32_MAX, ref_order, st, lstack, ltstack, ts);
+    rays++;
+    float* hp = w.hit;
+    hp[0 * cap + p] = h.z;
+    hp[1 * cap + p] = __uint_as_float(h.obj);
+    hp[2 * cap + p] = __uint_as_float(h.face);
+    hp[3 * cap + p] = h.b0;
+    hp[4 * cap + p] = h.b1;
+    hp[5 * cap + p] = h.b2;
+    hp[6 * cap + p] = h.pl.x;
+    hp[7 * cap + p] = h.pl.y;
+    hp[8 * cap + p] = h.pl.z;
+  }
+  flush_counters(cnt, rays, 0u, ts, 0u);
+}
+
+}  // namespace
+
+// ---- shade ------------------------------------------------------------------------
+
+template <int K>
+__global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveState w, DevCounters* cnt) {
+  uint32_t const n = *w.n_in;
+  uint32_t const cap = w.cap;
+  float const omega = S.lambda_sup - S.lambda_inf;
+  float const step = omega / float(K);
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t const i = base + threadIdx.x;
+    bool const live = i < n;
+    bool cont = false, shadow = false;
+    uint32_t p = 0;
+    f3 sp = f3{0.f, 0.f, 0.f}, sd = f3{0.f, 0.f, 1.f};
+    float stmax = 0.f;
+    uint32_t sskip = UINT32_MAX;
+    f3 nd = f3{0.f, 0.f, 1.f}, np = f3{0.f, 0.f, 0.f};
+    float lis_scale = 0.f, m_scale = 0.f;
+    if (live) {
+      p = w.q_in[i];
+      HitRec h;
+      h.obj = __float_as_uint(w.hit[cap + p]);
+      if (h.obj != UINT32_MAX) {
+        h.z = w.hit[p];
+        h.face = __float_as_uint(w.hit[2 * cap + p]);
+        h.b0 = w.hit[3 * cap + p];
+        h.b1 = w.hit[4 * cap + p];
+        h.b2 = w.hit[5 * cap + p];
+        h.pl = f3{w.hit[6 * cap + p], w.hit[7 * cap + p], w.hit[8 * cap + p]};
+        Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
+                               f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+        HitInfo const H = finalize_hit(S, r, h);
+        f3 const un = fnorm(r.u);
+        f3 const o = f3{-un.x, -un.y, -un.z};
+        f3 const nn = H.front ? H.F.z : neg3(H.F.z);
+        const DevMaterial& m = S.mats[H.mat];
+        float const hero = w.hero[p];
+        if (m.type == LGPU_MAT_EMITTER || m.type == LGPU_MAT_DIREMITTER) {
+          float g = 1.f;
+          if (m.type == LGPU_MAT_DIREMITTER) {
+            float const c = fdot(o, H.F.z);
+            g = powf(c >= 0.f ? c : 0.f, m.specular);
+          }
+          for (int k = 0; k < K; k++) {
+            float const x = lam_coord(S, hero_lambda(S, hero, step, k));
+            w.acc[k * cap + p] += w.beta[k * cap + p] * (spec_at(S, m.spectrum[0], x) * g);
+          }
+        } else if (w.depth[p] <= a.max_scatter) {
+          uint64_t rng = w.rng[p];
+          uint32_t const li = uint32_t(lgpu_u64(&rng) % uint64_t(S.n_lights));
+          float const prob_l = 1.f / float(S.n_lights);
+          const lgpu_light& L = S.lights[li];
+          // light sample without its visibility (the shadow kernel applies it)
+          LightSample ls = sample_light_unoccluded(S, L, H, rng, stmax, sskip);
+          float const x0 = lam_coord(S, hero);
+          BsdfScalars const bl = bsdf_scalars(S, m, x0, ls.dir, o, nn, H.front);
+          MatSample const ms = sample_material(S, m, x0, H, o, a.sample_p, rng);
+          float w_L = 1.f, w_mat = 0.f;
+          if (ms.ok) {
+            float const p_L_mati = prob_for_light(S, L, H.p, ms.dir) * prob_l;
+            float const p_mat_Li = prob_for_material(S, m, x0, H, ls.dir, o, a.sample_p);
+            float const p_L_i = ls.prob * prob_l;
+            w_L = p_L_i * p_L_i / (p_L_i * p_L_i + p_mat_Li * p_mat_Li);
+            w_mat = ms.prob * ms.prob / (ms.prob * ms.prob + p_L_mati * p_L_mati);
+          }
+          lis_scale = ls.scale / (ls.prob * prob_l) * w_L;
+          m_scale = ms.ok ? w_mat / ms.prob : 0.f;
+          bool const needs_test = stmax >= 0.f;
+          shadow = needs_test && lis_scale != 0.f;
+          for (int k = 0; k < K; k++) {
+            float const l = hero_lambda(S, hero, step, k);
+            float const x = lam_coord(S, l);
+            float const coef = bsdf_k(S, m, bl, x, l, H.front);
+            float const rad = spec_at(S, L.spectrum, x);
+            float const b = w.beta[k * cap + p];
+            float const contrib = b * (rad * coef * lis_scale);
+            if (!needs_test) w.acc[k * cap + p] += contrib;
+            else w.s_contrib[k * cap + p] = contrib;  // slot p; gathered via s_path
+            if (ms.ok) w.beta[k * cap + p] = b * (mat_mult_k(S, m, ms, x, l, H.front) * m_scale);
+          }
+          w.rng[p] = rng;
+          sp = H.p;
+          sd = ls.dir;
+          cont = ms.ok;
+          if (cont) {
+            np = H.p;
+            nd = ms.dir;
+          }
+        }
+      }
+    }
+    // compacted appends: next-bounce queue and shadow queue
+    uint32_t const qo = warp_append(w.n_out, cont);
+    if (cont) {
+      w.q_out[qo] = p;
+      w.ray[0 * cap + p] = np.x;
+      w.ray[1 * cap + p] = np.y;
+      w.ray[2 * cap + p] = np.z;
+      w.ray[3 * cap + p] = nd.x;
+      w.ray[4 * cap + p] = nd.y;
+      w.ray[5 * cap + p] = nd.z;
+      w.depth[p] += 1;
+    }
+    uint32_t const so = warp_append(w.n_shadow, shadow);
+    if (shadow) {
+      w.s_path[so] = p;
+      w.sray[0 * cap + so] = sp.x;
+      w.sray[1 * cap + so] = sp.y;
+      w.sray[2 * cap + so] = sp.z;
+      w.sray[3 * cap + so] = sd.x;
+      w.sray[4 * cap + so] = sd.y;
+      w.sray[5 * cap + so] = sd.z;
+      w.sray[6 * cap + so] = stmax;
+      w.sray[7 * cap + so] = __uint_as_float(sskip);
+    }
+  }
+  (void)cnt;
+}
+
+// ---- shadow -----------------------------------------------------------------------
+
+template <int K>
+__global__ void __launch_bounds__(128) wf_shadow(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
+  extern __shared__ StackEntry smem_stack[];
+  StackEntry lm[kLocalStack];
+  StackEntry lstack[kStackCap];
+  StackEntry ltstack[kTlasStackCap];
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  TravStats ts{0u, 0u, 0u, 0u};
+  uint32_t rays = 0;
+  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
+  uint32_t const n = *w.n_shadow;
+  uint32_t const cap = w.cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Ray const r = make_ray(f3{w.sray[i], w.sray[cap + i], w.sray[2 * cap + i]},
+                           f3{w.sray[3 * cap + i], w.sray[4 * cap + i], w.sray[5 * cap + i]});
+    HitRec h;
+    h.z = w.sray[6 * cap + i];
+    h.obj = UINT32_MAX;
+    uint32_t const skip = __float_as_uint(w.sray[7 * cap + i]);
+    bool const occ = scene_trace<true>(S, r, h, skip, ref_order, st, lstack, ltstack, ts);
+    rays++;
+    if (!occ) {
+      uint32_t const p = w.s_path[i];
+      for (int k = 0; k < K; k++) w.acc[k * cap + p] += w.s_contrib[k * cap + p];
+    }
+  }
+  flush_counters(cnt, rays, 0u, ts, 0u);
+}
+
+// ---- film ---------------------------------------------------------------------------
+
+template <int K>
+__global__ void __launch_bounds__(256) wf_splat(DevScene S, WaveState w, DevCounters* cnt) {
+  uint32_t nonfinite = 0;
+  float const omega = S.lambda_sup - S.lambda_inf;
+  float const step = omega / float(K);
+  float const prob_l = 1.f / omega;
+  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < w.npix; pix += gridDim.x * blockDim.x) {
+    float X = w.film[3 * pix], Y = w.film[3 * pix + 1], Z = w.film[3 * pix + 2];
+    for (uint32_t s = 0; s < w.n_samples; s++) {
+      uint32_t const p = s * w.npix + pix;
+      float const hero = w.hero[p];
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      bool finite = true;
+      for (int k = 0; k < K; k++) {
+        float const val = w.acc[k * w.cap + p] / prob_l;
+        finite = finite && isfinite(val);
+        splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
+      }
+      nonfinite += finite ? 0u : 1u;
+      X += sx;
+      Y += sy;
+      Z += sz;
+    }
+    w.film[3 * pix] = X;
+    w.film[3 * pix + 1] = Y;
+    w.film[3 * pix + 2] = Z;
+  }
+  TravStats const ts{0u, 0u, 0u, 0u};
+  flush_counters(cnt, 0u, 0u, ts, nonfinite);
+}
+
+}  // namespace lgpu

@@ -40,7 +40,9 @@ def _compare(g, o):
 
 
 @pytest.mark.parametrize("which,flags", [("mixed_nls", L.FLAG_REFERENCE_ORDER), ("mixed_nls", 0),
-                                         ("mixed2_nls", 0), ("box_nls", 0)])
+                                         ("mixed2_nls", 0), ("box_nls", 0),
+                                         ("mixed_nls", L.FLAG_MEGAKERNEL),
+                                         ("mixed2_nls", L.FLAG_MEGAKERNEL)])
 def test_render_matches_oracle_same_stream(which, flags, request):
     nls = request.getfixturevalue(which)
     sc = load_nls(nls)
