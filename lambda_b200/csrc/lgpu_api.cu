@@ -51,7 +51,7 @@ struct lgpu_ctx {
   // wavefront state (lgpu_wave.cuh), sized for the last frame rendered
   DevArray<float> w_ray, w_hero, w_beta, w_acc, w_hit, w_sray, w_scontrib, w_film;
   DevArray<uint64_t> w_rng;
-  DevArray<uint32_t> w_depth, w_q0, w_q1, w_spath, w_counts;
+  DevArray<uint32_t> w_depth, w_q0, w_q1, w_spath, w_counts, w_fb;
   uint32_t w_cap = 0, w_k = 0, w_npix = 0;
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
@@ -156,7 +156,8 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
     if (e == cudaSuccess) e = ensure(ctx->w_q0, c);
     if (e == cudaSuccess) e = ensure(ctx->w_q1, c);
     if (e == cudaSuccess) e = ensure(ctx->w_spath, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_counts, 4);
+    if (e == cudaSuccess) e = ensure(ctx->w_fb, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_counts, 8);
     if (e != cudaSuccess) {
       ctx->w_cap = 0;
       return cuda_fail(ctx, e, "wavefront buffers");
@@ -180,6 +181,9 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
   ws.n_in = ctx->w_counts.ptr;
   ws.n_out = ctx->w_counts.ptr + 1;
   ws.n_shadow = ctx->w_counts.ptr + 2;
+  ws.fetch = ctx->w_counts.ptr + 3;
+  ws.n_fb = ctx->w_counts.ptr + 5;
+  ws.fb_queue = ctx->w_fb.ptr;
   ws.sray = ctx->w_sray.ptr;
   ws.s_path = ctx->w_spath.ptr;
   ws.s_contrib = ctx->w_scontrib.ptr;
@@ -253,7 +257,8 @@ void lgpu_destroy(lgpu_ctx* ctx) {
                              &ctx->w_sray, &ctx->w_scontrib, &ctx->w_film})
     a->release();
   ctx->w_rng.release();
-  for (DevArray<uint32_t>* a : {&ctx->w_depth, &ctx->w_q0, &ctx->w_q1, &ctx->w_spath, &ctx->w_counts})
+  for (DevArray<uint32_t>* a : {&ctx->w_depth, &ctx->w_q0, &ctx->w_q1, &ctx->w_spath, &ctx->w_counts,
+                                &ctx->w_fb})
     a->release();
   ctx->rays.release();
   ctx->hits.release();

@@ -39,6 +39,9 @@ struct WaveState {
   uint32_t* s_path;  // cap
   float* s_contrib;  // K*cap
   uint32_t* n_shadow;
+  uint32_t* fetch;     // 2 work counters of the persistent trace kernels
+  uint32_t* fb_queue;  // extension rays re-traced in the reference's object order
+  uint32_t* n_fb;
   float* film;       // 3*npix XYZ
 };
 

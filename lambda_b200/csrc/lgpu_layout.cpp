@@ -53,17 +53,18 @@ struct BuildNode {
   }
 };
 
-constexpr size_t kPrimPerLeaf = 4;  // PRIM_PER_LEAF, cg.hpp:568
+constexpr size_t kPrimPerLeaf = 4;  // PRIM_PER_LEAF, cg.hpp:568 (meshes)
 
 struct Builder {
   const PrimBox* boxes;
   const float* cent;
+  size_t max_leaf;
   uint32_t n_nodes = 0, n_interior = 0;
 
   // bvh::splitbuildnode (cg.hpp:632-683)
   void split(BuildNode* node) {
     n_nodes++;
-    if (node->prims.size() <= kPrimPerLeaf) {
+    if (node->prims.size() <= max_leaf) {
       node->leaf = true;
       return;
     }
@@ -107,7 +108,8 @@ struct Builder {
 
 }  // namespace
 
-void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out) {
+void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out,
+                   size_t max_leaf) {
   out = RefBvh{};
   if (n == 0) return;
   PrimBox bb;
@@ -118,7 +120,7 @@ void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
     all[i] = i;
   }
   std::unique_ptr<BuildNode> root(new BuildNode(bb, std::move(all)));
-  Builder B{boxes, centroids};
+  Builder B{boxes, centroids, max_leaf};
   B.split(root.get());
   out.n_nodes = B.n_nodes;
   out.n_interior = B.n_interior;
@@ -476,7 +478,8 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
   }
   if (sc.n_objects > 0) {
     RefBvh tl;
-    build_ref_bvh(sc.n_objects, boxes.data(), cents.data(), tl);
+    // one object per leaf: objects are culled by the 8-wide box test
+    build_ref_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
     L.tlas_objects = tl.prim_idxs;
     RefView const R{tl.n_nodes, uint32_t(tl.bbs.size() / 48), uint32_t(tl.prim_idxs.size()),
                     tl.nodes.data(), tl.bbs.data(), tl.prim_idxs.data()};

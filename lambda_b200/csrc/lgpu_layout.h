@@ -23,8 +23,10 @@ struct PrimBox {
 };
 
 // Builds over n primitives given their boxes and centroids
-// (centroid[3*i + axis]).
-void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out);
+// (centroid[3*i + axis]); leaves hold at most max_leaf primitives (the
+// reference's PRIM_PER_LEAF = 4 for meshes).
+void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out,
+                   size_t max_leaf = 4);
 
 // Boxes and centroids of triangle faces as trimeshdata::aabboftri and
 // centroidoftri compute them (cg.hpp:776-790).

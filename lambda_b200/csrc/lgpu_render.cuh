@@ -105,15 +105,25 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
   }
   WaveState w = *wave;
   size_t const smem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
-  static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0;
+  static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0, g_ptrace = 0, g_pshadow = 0,
+                  g_fb = 0;
   if (!g_trace) {
     cudaFuncSetAttribute(wf_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(wf_shadow<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(wf_trace_persistent<false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(smem));
+    cudaFuncSetAttribute(wf_trace_persistent<true, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         int(smem));
     g_trace = persistent_blocks(wf_trace, 128, smem);
     g_shadow = persistent_blocks(wf_shadow<K>, 128, smem);
+    g_ptrace = persistent_blocks(wf_trace_persistent<false, K>, 128, smem);
+    g_pshadow = persistent_blocks(wf_trace_persistent<true, K>, 128, smem);
     g_shade = persistent_blocks(wf_shade<K>, 128, 0);
     g_gen = persistent_blocks(wf_generate, 256, 0);
+    g_fb = persistent_blocks(wf_trace_fallback, 128, 0);
   }
+  // the instance BVH kernels, or the reference's linear object loop
+  bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
   uint32_t const per_wave = w.n_samples;
   for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += per_wave) {
@@ -122,10 +132,16 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
     // a path scatters at most max_scatter+1 times: max_scatter+2 segments
     for (uint32_t b = 0; b < a.max_scatter + 2; b++) {
       cudaMemsetAsync(w.n_out, 0, sizeof(uint32_t), st);
-      cudaMemsetAsync(w.n_shadow, 0, sizeof(uint32_t), st);
-      wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      cudaMemsetAsync(w.n_shadow, 0, 4 * sizeof(uint32_t), st);  // n_shadow, fetch[2], n_fb
+      if (linear) {
+        wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      } else {
+        wf_trace_persistent<false, K><<<g_ptrace, 128, smem, st>>>(S, w, d_cnt);
+        wf_trace_fallback<<<g_fb, 128, 0, st>>>(S, w, d_cnt);
+      }
       wf_shade<K><<<g_shade, 128, 0, st>>>(S, a, w, d_cnt);
-      wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      if (linear) wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, d_cnt);
+      else wf_trace_persistent<true, K><<<g_pshadow, 128, smem, st>>>(S, w, d_cnt);
       uint32_t* t = w.q_in;
       w.q_in = w.q_out;
       w.q_out = t;

@@ -191,6 +191,140 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
   return hit_any;
 }
 
+// trace_tlas as a resumable state machine: trace_begin sets up a ray,
+// trace_step processes one stack entry.  The persistent trace kernels call
+// trace_step in a loop shared by the whole warp and give a lane a new ray
+// as soon as its ray is finished, so lanes do not idle while the longest ray
+// of their warp completes.
+struct TraceState {
+  Ray w, l;
+  f3 mr;
+  HitRec h;
+  uint32_t skip, cur;
+  float zs, cur_exit;
+  bool in_mesh, lowered, cur_inside, hit_any;
+};
+
+__device__ __forceinline__ void trace_begin(const DevScene& S, TraceState& t, SplitStack& st) {
+  t.h.inside = false;
+  t.in_mesh = t.lowered = t.cur_inside = t.hit_any = false;
+  t.cur = 0;
+  t.zs = t.cur_exit = 0.f;
+  st.sp = 0;
+  float const t0 = segment_box_entry(S.tlas_bounds, t.w, t.h.z);
+  if (t0 != kFltMax) st.push(StackEntry{S.tlas_root, t0});
+}
+
+// One step of trace_tlas; returns true when the ray is finished (stack
+// empty, or ANY and a hit was found).
+template <bool ANY>
+__device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, SplitStack& st,
+                                           TravStats& ts) {
+  if (st.sp == 0) return true;
+  StackEntry const e = st.pop();
+  HitRec& h = t.h;
+  if (e.ref == kMarker) {
+    t.in_mesh = false;
+    if (t.lowered && h.obj != t.cur) h.z = t.zs;
+    t.lowered = false;
+    return st.sp == 0;
+  }
+  if (e.t > h.z) return st.sp == 0;
+  if (!(e.ref & kLeafBit)) {
+    ts.nodes++;
+    if (!push_children_split(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st)) {
+      ts.flags |= 1u;
+      return true;
+    }
+    return st.sp == 0;
+  }
+  uint32_t const cnt = ((e.ref >> 28) & 7u) + 1u;
+  uint32_t const slot = e.ref & kSlotMask;
+  if (t.in_mesh) {
+    for (uint32_t k = 0; k < cnt; k++) {
+      const TriSlot& T = S.tris[slot + k];
+      ts.tris++;
+      float tt, b0, b1, b2;
+      if (tri_test(T, t.l, t.mr, h.z, tt, b0, b1, b2)) {
+        h.z = tt;
+        h.obj = t.cur;
+        h.face = __float_as_uint(T.v0[3]);
+        h.b0 = b0;
+        h.b1 = b1;
+        h.b2 = b2;
+        h.pl = ray_at(t.l, tt);
+        h.inside = t.cur_inside;
+        h.exit = t.cur_exit;
+        t.hit_any = true;
+        if (ANY) return true;
+      }
+    }
+    return st.sp == 0;
+  }
+  uint32_t const i = S.tlas_objects[slot];
+  if (cnt > 1) {
+    if (st.sp + 1 > kSplitCap) {
+      ts.flags |= 1u;
+      return true;
+    }
+    st.push(StackEntry{kLeafBit | ((cnt - 2u) << 28) | (slot + 1u), e.t});
+  }
+  if (i == t.skip) return st.sp == 0;
+  ts.insts++;
+  const DevObject& ob = S.objects[i];
+  bool const low = !ANY && h.obj != UINT32_MAX && i < h.obj;
+  float const z_saved = h.z;
+  if (low) h.z = prev_float(z_saved);
+  Ray const li = to_local(ob, t.w);
+  if (ob.type != LGPU_OBJ_TRIMESH) {
+    float tt;
+    f3 x;
+    bool hit;
+    if (ob.type == LGPU_OBJ_SPHERE) {
+      hit = sphere_test(li, h.z, tt);
+      if (hit) x = ray_at(li, tt);
+    } else {
+      hit = plane_test(li, h.z, tt, x);
+    }
+    if (hit) {
+      h.z = tt;
+      h.obj = i;
+      h.face = UINT32_MAX;
+      h.pl = x;
+      h.inside = false;
+      t.hit_any = true;
+      if (ANY) return true;
+    } else if (low) {
+      h.z = z_saved;
+    }
+    return st.sp == 0;
+  }
+  const DevMesh& m = S.meshes[ob.mesh];
+  bool inside;
+  float ex;
+  float r0 = aabb_scalar(m.bounds, li, h.z, inside, ex);
+  if (r0 != kFltMax && !ANY && inside) r0 = kBias;
+  if (r0 == kFltMax || r0 > h.z) {
+    if (low) h.z = z_saved;
+    return st.sp == 0;
+  }
+  if (st.sp + 2 > kSplitCap) {
+    ts.flags |= 1u;
+    return true;
+  }
+  t.l = li;
+  t.mr = cross3(li.p, li.u);
+  t.cur = i;
+  t.cur_inside = inside;
+  t.cur_exit = ex;
+  t.zs = z_saved;
+  t.lowered = low;
+  t.in_mesh = true;
+  st.push(StackEntry{kMarker, 0.f});
+  st.push(StackEntry{m.root, r0});
+  return false;
+}
+
 // intersect::scene for the wavefront kernels: the instance BVH through
 // trace_tlas, the reference's linear object loop (nested traversal, local
 // stack) for reference order, tiny scenes and the order-dependent case.

@@ -136,6 +136,129 @@ __global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 
+// Persistent instance-BVH traversal of the extension rays (ANY = false,
+// queue q_in, hit records out) or the shadow rays (ANY = true, shadow
+// queue, unoccluded contributions added to the path radiance).  A lane that
+// finishes its ray takes the next one; idle lanes are refilled together with
+// one atomic per warp once kRefill of them are waiting.
+constexpr int kRefill = 8;
+
+template <bool ANY, int K>
+__global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveState w, DevCounters* cnt) {
+  extern __shared__ StackEntry smem_stack[];
+  StackEntry lm[kLocalStack];
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  TravStats ts{0u, 0u, 0u, 0u};
+  uint32_t rays = 0;
+  uint32_t const n = ANY ? *w.n_shadow : *w.n_in;
+  uint32_t* fetch = ANY ? w.fetch + 1 : w.fetch;
+  uint32_t const cap = w.cap;
+  unsigned const FULL = 0xFFFFFFFFu;
+  int const lane = threadIdx.x & 31;
+  TraceState t;
+  bool active = false, exhausted = false;
+  uint32_t idx = 0;
+  while (true) {
+    unsigned const idle = __ballot_sync(FULL, !active);
+    if (!exhausted && (__popc(idle) >= kRefill || idle == FULL)) {
+      int const leader = __ffs(idle) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(fetch, uint32_t(__popc(idle)));
+      base = __shfl_sync(FULL, base, leader);
+      if (base + uint32_t(__popc(idle)) >= n) exhausted = true;
+      if (!active) {
+        uint32_t const my = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
+        if (my < n) {
+          idx = my;
+          if (ANY) {
+            t.w = make_ray(f3{w.sray[my], w.sray[cap + my], w.sray[2 * cap + my]},
+                           f3{w.sray[3 * cap + my], w.sray[4 * cap + my], w.sray[5 * cap + my]});
+            t.h.z = w.sray[6 * cap + my];
+            t.skip = __float_as_uint(w.sray[7 * cap + my]);
+          } else {
+            uint32_t const p = w.q_in[my];
+            idx = p;
+            t.w = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
+                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+            t.h.z = kFltMax;
+            t.skip = UINT32_MAX;
+          }
+          t.h.obj = UINT32_MAX;
+          t.h.face = UINT32_MAX;
+          t.h.b0 = t.h.b1 = t.h.b2 = 0.f;
+          t.h.pl = f3{0.f, 0.f, 0.f};
+          trace_begin(S, t, st);
+          active = true;
+          rays++;
+        }
+      }
+    }
+    if (__all_sync(FULL, !active)) {
+      if (exhausted) break;
+      continue;
+    }
+    if (active && trace_step<ANY>(S, t, st, ts)) {
+      active = false;
+      if (ANY) {
+        if (!t.hit_any) {
+          uint32_t const p = w.s_path[idx];
+          for (int k = 0; k < K; k++) w.acc[k * cap + p] += w.s_contrib[k * cap + p];
+        }
+      } else if (t.hit_any && t.h.inside && t.h.exit > t.h.z) {
+        // the reference's object order could change this hit: redo the ray
+        // with the linear object loop (wf_trace_fallback)
+        w.fb_queue[atomicAdd(w.n_fb, 1u)] = idx;
+      } else {
+        uint32_t const p = idx;
+        float* hp = w.hit;
+        hp[0 * cap + p] = t.h.z;
+        hp[1 * cap + p] = __uint_as_float(t.h.obj);
+        hp[2 * cap + p] = __uint_as_float(t.h.face);
+        hp[3 * cap + p] = t.h.b0;
+        hp[4 * cap + p] = t.h.b1;
+        hp[5 * cap + p] = t.h.b2;
+        hp[6 * cap + p] = t.h.pl.x;
+        hp[7 * cap + p] = t.h.pl.y;
+        hp[8 * cap + p] = t.h.pl.z;
+      }
+    }
+  }
+  flush_counters(cnt, rays, 0u, ts, 0u);
+}
+
+// Extension rays whose closest hit depends on the reference's object order
+// (see scene_hit): the linear object loop.
+__global__ void __launch_bounds__(128) wf_trace_fallback(DevScene S, WaveState w, DevCounters* cnt) {
+  StackEntry lstack[kStackCap];
+  StackEntry ltstack[kTlasStackCap];
+  TravStats ts{0u, 0u, 0u, 0u};
+  uint32_t const n = *w.n_fb;
+  uint32_t const cap = w.cap;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t const p = w.fb_queue[i];
+    Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
+                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+    HitRec h;
+    h.z = kFltMax;
+    h.obj = UINT32_MAX;
+    h.face = UINT32_MAX;
+    h.b0 = h.b1 = h.b2 = 0.f;
+    h.pl = f3{0.f, 0.f, 0.f};
+    scene_hit<false>(S, r, h, UINT32_MAX, true, lstack, ltstack, ts);
+    float* hp = w.hit;
+    hp[0 * cap + p] = h.z;
+    hp[1 * cap + p] = __uint_as_float(h.obj);
+    hp[2 * cap + p] = __uint_as_float(h.face);
+    hp[3 * cap + p] = h.b0;
+    hp[4 * cap + p] = h.b1;
+    hp[5 * cap + p] = h.b2;
+    hp[6 * cap + p] = h.pl.x;
+    hp[7 * cap + p] = h.pl.y;
+    hp[8 * cap + p] = h.pl.z;
+  }
+  flush_counters(cnt, 0u, 0u, ts, 0u);
+}
+
 }  // namespace
 
 // ---- shade ------------------------------------------------------------------------
