@@ -330,6 +330,7 @@ def main():
     ap.add_argument("--impl", default="lgpu", choices=["lgpu", "reference"])
     ap.add_argument("--small", action="store_true", help="reduced frame (profiling)")
     ap.add_argument("--spp", type=int, default=None)
+    ap.add_argument("--width", type=int, default=None, help="frame width (profiling)")
     ap.add_argument("--no-baseline", action="store_true")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="seconds of reference CPU work per sampled step")
@@ -337,6 +338,8 @@ def main():
     w = dict(SMALL if args.small else FULL)
     if args.spp:
         w["spp"] = args.spp
+    if args.width:
+        w["width"] = args.width
     if args.impl == "reference":
         return run_reference(args, w)
     return run_device(args, w)

@@ -38,9 +38,11 @@ struct SplitStack {
 
 constexpr int kSplitCap = kSmemStack + kLocalStack;
 
-// push_children (lgpu_intersect.cuh) writing through a SplitStack
+// push_children (lgpu_intersect.cuh) writing through a SplitStack.  With
+// `sorted` false (any-hit queries, whose boolean answer does not depend on
+// the visiting order) the hit children are pushed in child order.
 __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ray& r, float t_max,
-                                                    SplitStack& st) {
+                                                    SplitStack& st, bool sorted) {
   bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
   float t[8];
   uint32_t ref[8];
@@ -53,6 +55,12 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
 #pragma unroll
   for (int c = 0; c < 8; c++) hits += (t[c] != 0.f) ? 1 : 0;
   if (st.sp + hits > kSplitCap) return false;
+  if (!sorted) {
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      if (t[c] != 0.f) st.push(StackEntry{ref[c], t[c]});
+    return true;
+  }
 #pragma unroll
   for (int c = 0; c < 8; c++) {
     if (t[c] == 0.f) continue;
@@ -96,7 +104,7 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
     if (e.t > h.z) continue;
     if (!(e.ref & kLeafBit)) {
       ts.nodes++;
-      if (!push_children_split(S.nodes[e.ref], in_mesh ? l : w, h.z, st)) {
+      if (!push_children_split(S.nodes[e.ref], in_mesh ? l : w, h.z, st, !ANY)) {
         ts.flags |= 1u;
         break;
       }
@@ -196,19 +204,25 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
 // trace_step in a loop shared by the whole warp and give a lane a new ray
 // as soon as its ray is finished, so lanes do not idle while the longest ray
 // of their warp completes.
+// Besides the ray, a query has a mode (`any`: stop at the first hit, as
+// shadow rays do), an object to skip and an index limit (objects with a
+// higher or equal index are ignored), and counts the meshes whose bounds
+// contain the ray origin (n_inside).
 struct TraceState {
   Ray w, l;
   f3 mr;
   HitRec h;
-  uint32_t skip, cur;
+  uint32_t skip, ilimit, cur;
   float zs, cur_exit;
-  bool in_mesh, lowered, cur_inside, hit_any;
+  uint32_t n_inside;
+  bool any, in_mesh, lowered, cur_inside, hit_any;
 };
 
 __device__ __forceinline__ void trace_begin(const DevScene& S, TraceState& t, SplitStack& st) {
   t.h.inside = false;
   t.in_mesh = t.lowered = t.cur_inside = t.hit_any = false;
   t.cur = 0;
+  t.n_inside = 0;
   t.zs = t.cur_exit = 0.f;
   st.sp = 0;
   float const t0 = segment_box_entry(S.tlas_bounds, t.w, t.h.z);
@@ -216,11 +230,13 @@ __device__ __forceinline__ void trace_begin(const DevScene& S, TraceState& t, Sp
 }
 
 // One step of trace_tlas; returns true when the ray is finished (stack
-// empty, or ANY and a hit was found).
+// empty, or an any-hit query found a hit).  ANY fixes the mode at compile
+// time; otherwise t.any selects it.
 template <bool ANY>
 __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, SplitStack& st,
                                            TravStats& ts) {
   if (st.sp == 0) return true;
+  bool const any = ANY || t.any;
   StackEntry const e = st.pop();
   HitRec& h = t.h;
   if (e.ref == kMarker) {
@@ -232,7 +248,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   if (e.t > h.z) return st.sp == 0;
   if (!(e.ref & kLeafBit)) {
     ts.nodes++;
-    if (!push_children_split(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st)) {
+    if (!push_children_split(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
       ts.flags |= 1u;
       return true;
     }
@@ -256,7 +272,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
         h.inside = t.cur_inside;
         h.exit = t.cur_exit;
         t.hit_any = true;
-        if (ANY) return true;
+        if (any) return true;
       }
     }
     return st.sp == 0;
@@ -269,10 +285,10 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
     }
     st.push(StackEntry{kLeafBit | ((cnt - 2u) << 28) | (slot + 1u), e.t});
   }
-  if (i == t.skip) return st.sp == 0;
+  if (i == t.skip || i >= t.ilimit) return st.sp == 0;
   ts.insts++;
   const DevObject& ob = S.objects[i];
-  bool const low = !ANY && h.obj != UINT32_MAX && i < h.obj;
+  bool const low = !any && h.obj != UINT32_MAX && i < h.obj;
   float const z_saved = h.z;
   if (low) h.z = prev_float(z_saved);
   Ray const li = to_local(ob, t.w);
@@ -293,7 +309,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
       h.pl = x;
       h.inside = false;
       t.hit_any = true;
-      if (ANY) return true;
+      if (any) return true;
     } else if (low) {
       h.z = z_saved;
     }
@@ -303,7 +319,8 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   bool inside;
   float ex;
   float r0 = aabb_scalar(m.bounds, li, h.z, inside, ex);
-  if (r0 != kFltMax && !ANY && inside) r0 = kBias;
+  if (r0 != kFltMax && inside) t.n_inside++;
+  if (r0 != kFltMax && !any && inside) r0 = kBias;
   if (r0 == kFltMax || r0 > h.z) {
     if (low) h.z = z_saved;
     return st.sp == 0;

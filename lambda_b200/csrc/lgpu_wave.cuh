@@ -143,6 +143,20 @@ __global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_
 // one atomic per warp once kRefill of them are waiting.
 constexpr int kRefill = 8;
 
+__device__ __forceinline__ void store_hit(const WaveState& w, uint32_t p, const HitRec& h) {
+  uint32_t const cap = w.cap;
+  float* hp = w.hit;
+  hp[0 * cap + p] = h.z;
+  hp[1 * cap + p] = __uint_as_float(h.obj);
+  hp[2 * cap + p] = __uint_as_float(h.face);
+  hp[3 * cap + p] = h.b0;
+  hp[4 * cap + p] = h.b1;
+  hp[5 * cap + p] = h.b2;
+  hp[6 * cap + p] = h.pl.x;
+  hp[7 * cap + p] = h.pl.y;
+  hp[8 * cap + p] = h.pl.z;
+}
+
 template <bool ANY, int K>
 __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
@@ -157,7 +171,8 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
   int const lane = threadIdx.x & 31;
   TraceState t;
   bool active = false, exhausted = false;
-  uint32_t idx = 0;
+  uint32_t idx = 0, wobj = 0;
+  int phase = 1;
   while (true) {
     unsigned const idle = __ballot_sync(FULL, !active);
     if (!exhausted && (__popc(idle) >= kRefill || idle == FULL)) {
@@ -187,6 +202,9 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
           t.h.face = UINT32_MAX;
           t.h.b0 = t.h.b1 = t.h.b2 = 0.f;
           t.h.pl = f3{0.f, 0.f, 0.f};
+          t.any = ANY;
+          t.ilimit = UINT32_MAX;
+          phase = 1;
           trace_begin(S, t, st);
           active = true;
           rays++;
@@ -204,23 +222,52 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
           uint32_t const p = w.s_path[idx];
           for (int k = 0; k < K; k++) w.acc[k * cap + p] += w.s_contrib[k * cap + p];
         }
-      } else if (t.hit_any && t.h.inside && t.h.exit > t.h.z) {
-        // the reference's object order could change this hit: redo the ray
-        // with the linear object loop (wf_trace_fallback)
-        w.fb_queue[atomicAdd(w.n_fb, 1u)] = idx;
-      } else {
-        uint32_t const p = idx;
-        float* hp = w.hit;
-        hp[0 * cap + p] = t.h.z;
-        hp[1 * cap + p] = __uint_as_float(t.h.obj);
-        hp[2 * cap + p] = __uint_as_float(t.h.face);
-        hp[3 * cap + p] = t.h.b0;
-        hp[4 * cap + p] = t.h.b1;
-        hp[5 * cap + p] = t.h.b2;
-        hp[6 * cap + p] = t.h.pl.x;
-        hp[7 * cap + p] = t.h.pl.y;
-        hp[8 * cap + p] = t.h.pl.z;
+        continue;
       }
+      uint32_t const p = idx;
+      if (phase == 2) {
+        // an object below W's index is hit before the ray leaves W's bounds:
+        // the reference skips W, so its answer is the closest hit without W
+        if (t.hit_any) {
+          t.w = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
+                         f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+          t.h.z = kFltMax;
+          t.h.obj = UINT32_MAX;
+          t.h.face = UINT32_MAX;
+          t.any = false;
+          t.skip = wobj;
+          t.ilimit = UINT32_MAX;
+          phase = 3;
+          trace_begin(S, t, st);
+          active = true;
+        }
+        continue;
+      }
+      if (phase == 1 && t.hit_any && t.h.inside && t.h.exit > t.h.z) {
+        // The winner W is a mesh whose bounds contain the ray origin and
+        // which the ray leaves after the hit; the reference skips W if an
+        // object tested before it (lower index) was hit before that exit
+        // (cg.hpp:1393, 1414).  With W the only such mesh, one any-hit query
+        // over the lower-index objects up to the exit decides it; otherwise
+        // the ray is re-traced with the linear object loop.
+        if (t.n_inside != 1) {
+          w.fb_queue[atomicAdd(w.n_fb, 1u)] = p;
+          continue;
+        }
+        store_hit(w, p, t.h);
+        wobj = t.h.obj;
+        float const ex = t.h.exit;
+        t.h.z = prev_float(ex);
+        t.h.obj = UINT32_MAX;
+        t.any = true;
+        t.skip = UINT32_MAX;
+        t.ilimit = wobj;
+        phase = 2;
+        trace_begin(S, t, st);
+        active = true;
+        continue;
+      }
+      store_hit(w, p, t.h);
     }
   }
   flush_counters(cnt, rays, 0u, ts, 0u);
