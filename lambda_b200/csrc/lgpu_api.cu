@@ -52,7 +52,10 @@ struct lgpu_ctx {
   DevArray<float> w_ray, w_hero, w_beta, w_acc, w_hit, w_sray, w_scontrib, w_film;
   DevArray<uint64_t> w_rng;
   DevArray<uint32_t> w_depth, w_q0, w_q1, w_spath, w_counts, w_fb;
-  uint32_t w_cap = 0, w_k = 0, w_npix = 0;
+  DevArray<uint32_t> w_pix, w_samp, w_free, w_fin, w_ctl;
+  DevArray<float> w_sbuf;
+  uint32_t* h_ctl = nullptr;  // pinned
+  uint32_t w_cap = 0, w_k = 0, w_npix = 0, w_chunk = 0;
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
   DevArray<double> partials;
@@ -139,9 +142,13 @@ int collect(lgpu_ctx* ctx, const char* what) {
 // Sizes the wavefront buffers for a frame of npix pixels and fills ws.
 int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
   uint32_t const K = ctx->S.hero_k;
-  uint32_t const ns = wave_samples(npix, spp);
-  uint32_t const cap = npix * ns;
-  if (cap != ctx->w_cap || K != ctx->w_k || npix != ctx->w_npix) {
+  // paths in flight: about 2^21, fewer for small frames
+  uint64_t const work = uint64_t(npix) * spp;
+  uint32_t const cap = uint32_t(work < (1u << 21) ? work : (1u << 21));
+  // samples per chunk: the (sample, pixel) film buffer stays under 2 GiB
+  uint64_t const max_ns = (uint64_t(1) << 31) / (12ull * npix);
+  uint32_t const ns = uint32_t(spp < max_ns ? spp : (max_ns ? max_ns : 1));
+  if (cap != ctx->w_cap || K != ctx->w_k || npix != ctx->w_npix || ns != ctx->w_chunk) {
     size_t const c = cap;
     cudaError_t e = ensure(ctx->w_ray, 6 * c);
     if (e == cudaSuccess) e = ensure(ctx->w_hero, c);
@@ -158,6 +165,12 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
     if (e == cudaSuccess) e = ensure(ctx->w_spath, c);
     if (e == cudaSuccess) e = ensure(ctx->w_fb, c);
     if (e == cudaSuccess) e = ensure(ctx->w_counts, 8);
+    if (e == cudaSuccess) e = ensure(ctx->w_pix, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_samp, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_free, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_fin, c);
+    if (e == cudaSuccess) e = ensure(ctx->w_ctl, 8);
+    if (e == cudaSuccess) e = ensure(ctx->w_sbuf, 3 * size_t(npix) * ns);
     if (e != cudaSuccess) {
       ctx->w_cap = 0;
       return cuda_fail(ctx, e, "wavefront buffers");
@@ -165,10 +178,18 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
     ctx->w_cap = cap;
     ctx->w_k = K;
     ctx->w_npix = npix;
+    ctx->w_chunk = ns;
   }
   ws.cap = cap;
   ws.npix = npix;
   ws.n_samples = ns;
+  ws.pix = ctx->w_pix.ptr;
+  ws.samp = ctx->w_samp.ptr;
+  ws.free_list = ctx->w_free.ptr;
+  ws.fin_list = ctx->w_fin.ptr;
+  ws.ctl = ctx->w_ctl.ptr;
+  ws.h_ctl = ctx->h_ctl;
+  ws.sbuf = ctx->w_sbuf.ptr;
   ws.ray = ctx->w_ray.ptr;
   ws.rng = ctx->w_rng.ptr;
   ws.hero = ctx->w_hero.ptr;
@@ -239,6 +260,7 @@ int lgpu_create(int device, lgpu_ctx** out) {
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, sizeof(DevCounters));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->exposure, sizeof(float));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, 8 * sizeof(uint32_t));
   if (e != cudaSuccess) {
     lgpu_destroy(ctx);
     return e == cudaErrorMemoryAllocation ? LGPU_ERR_OUT_OF_MEMORY : LGPU_ERR_CUDA;
@@ -258,8 +280,11 @@ void lgpu_destroy(lgpu_ctx* ctx) {
     a->release();
   ctx->w_rng.release();
   for (DevArray<uint32_t>* a : {&ctx->w_depth, &ctx->w_q0, &ctx->w_q1, &ctx->w_spath, &ctx->w_counts,
-                                &ctx->w_fb})
+                                &ctx->w_fb, &ctx->w_pix, &ctx->w_samp, &ctx->w_free, &ctx->w_fin,
+                                &ctx->w_ctl})
     a->release();
+  ctx->w_sbuf.release();
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   ctx->rays.release();
   ctx->hits.release();
   ctx->partials.release();

@@ -42,6 +42,17 @@ struct WaveState {
   uint32_t* fetch;     // 2 work counters of the persistent trace kernels
   uint32_t* fb_queue;  // extension rays re-traced in the reference's object order
   uint32_t* n_fb;
+  // streaming: a slot whose path ends is refilled with the next
+  // (sample, pixel) of the frame
+  uint32_t* pix;        // cap: pixel of the slot's path
+  uint32_t* samp;       // cap: sample index (relative to the chunk)
+  uint32_t* free_list;  // cap
+  uint32_t* fin_list;   // cap: slots whose path ended this iteration
+  uint32_t* ctl;        // [0] free slots, [1] next work item, [2] ended paths,
+                        // [3..6] plan of the next generate (new, first item,
+                        // free-list top, queue position)
+  uint32_t* h_ctl;      // pinned host copy of ctl[0..2] and the queue count
+  float* sbuf;          // 3 * npix * n_samples: XYZ of every (sample, pixel)
   float* film;       // 3*npix XYZ
 };
 

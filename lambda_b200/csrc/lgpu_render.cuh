@@ -125,12 +125,21 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
   // the instance BVH kernels, or the reference's linear object loop
   bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
-  uint32_t const per_wave = w.n_samples;
-  for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += per_wave) {
-    w.n_samples = (a.spp - s0 < per_wave) ? (a.spp - s0) : per_wave;
-    wf_generate<<<g_gen, 256, 0, st>>>(S, a, w, K, s0, d_cnt);
-    // a path scatters at most max_scatter+1 times: max_scatter+2 segments
-    for (uint32_t b = 0; b < a.max_scatter + 2; b++) {
+  // Streaming: every iteration ends paths (finish), starts new ones in the
+  // freed slots (plan + generate), then advances every path in flight by
+  // one segment (trace, shade, shadow).  The frame's samples are processed
+  // in chunks of w.n_samples (the size of the (sample, pixel) film buffer).
+  uint32_t const chunk = w.n_samples;
+  uint32_t const g_fin = g_gen;
+  for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
+    uint32_t const ns = (a.spp - s0 < chunk) ? (a.spp - s0) : chunk;
+    uint32_t const total = ns * w.npix;
+    wf_stream_init<<<g_gen, 256, 0, st>>>(w);
+    for (uint32_t it = 0;; it++) {
+      wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
+      cudaMemsetAsync(w.ctl + 2, 0, sizeof(uint32_t), st);
+      wf_plan<<<1, 1, 0, st>>>(w, total);
+      wf_generate_stream<<<g_gen, 256, 0, st>>>(S, a, w, K, s0, d_cnt);
       cudaMemsetAsync(w.n_out, 0, sizeof(uint32_t), st);
       cudaMemsetAsync(w.n_shadow, 0, 4 * sizeof(uint32_t), st);  // n_shadow, fetch[2], n_fb
       if (linear) {
@@ -148,11 +157,21 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
       t = w.n_in;
       w.n_in = w.n_out;
       w.n_out = t;
+      // look at the counters every few iterations: done when every work
+      // item was started and no path is in flight
+      if ((it & 3) == 3) {
+        cudaMemcpyAsync(w.h_ctl, w.ctl, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(w.h_ctl + 3, w.n_in, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) break;
+        if (w.h_ctl[1] == total && w.h_ctl[3] == 0) break;
+      }
     }
-    wf_splat<K><<<(w.npix + 255) / 256, 256, 0, st>>>(S, w, d_cnt);
+    if (e != cudaSuccess) break;
+    wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
+    wf_reduce<<<(w.npix + 255) / 256, 256, 0, st>>>(w, ns);
     e = cudaGetLastError();
   }
-  w.n_samples = per_wave;
   if (e == cudaSuccess) e = launch_finalize(w.film, w.npix, uint32_t(S.cam.width), uint32_t(S.cam.height),
                                             float(a.spp) * float(K), S.lambda_delta, d_out, st);
   return e;

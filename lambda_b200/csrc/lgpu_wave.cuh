@@ -136,6 +136,145 @@ __global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 
+// ---- streaming scheduler ------------------------------------------------------------
+
+// All slots free, no work handed out, no path in flight.
+__global__ void wf_stream_init(WaveState w) {
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < w.cap; p += gridDim.x * blockDim.x)
+    w.free_list[p] = p;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    w.ctl[0] = w.cap;
+    w.ctl[1] = 0;
+    w.ctl[2] = 0;
+    *w.n_in = 0;
+  }
+}
+
+// Decides how many new paths the next generate starts: as many as there
+// are free slots, up to the remaining work items.
+__global__ void wf_plan(WaveState w, uint32_t total) {
+  uint32_t const n_free = w.ctl[0], next = w.ctl[1];
+  uint32_t const left = total - next;
+  uint32_t const n_new = n_free < left ? n_free : left;
+  w.ctl[3] = n_new;
+  w.ctl[4] = next;
+  w.ctl[5] = n_free;
+  w.ctl[6] = *w.n_in;
+  w.ctl[0] = n_free - n_new;
+  w.ctl[1] = next + n_new;
+  *w.n_in += n_new;
+}
+
+// Starts the planned paths: work item q is sample q / npix of pixel
+// q % npix (all pixels of one sample before the next sample).
+__global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs a, WaveState w,
+                                                          uint32_t k_hero, uint32_t sample_base,
+                                                          DevCounters* cnt) {
+  uint32_t const n_new = w.ctl[3], first = w.ctl[4], top = w.ctl[5], qpos = w.ctl[6];
+  uint32_t paths = 0;
+  float const omega = S.lambda_sup - S.lambda_inf;
+  const lgpu_camera& C = S.cam;
+  uint32_t const W = uint32_t(C.width);
+  uint32_t const cap = w.cap;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_new; k += gridDim.x * blockDim.x) {
+    uint32_t const q = first + k;
+    uint32_t const s_local = q / w.npix;
+    uint32_t const pix = q - s_local * w.npix;
+    uint32_t const p = w.free_list[top - 1 - k];
+    uint32_t const i = pix / W, j = pix - i * W;
+    uint64_t rng = lgpu_path_state(a.seed, (uint64_t(a.stream_tag) << 32) | pix,
+                                   uint64_t(a.spp_offset) + sample_base + s_local);
+    float const u = float(j) + lgpu_flt(&rng);
+    float const v = float(i) + lgpu_flt(&rng);
+    f3 const Fx = f3{C.base_x[0], C.base_x[1], C.base_x[2]};
+    f3 const Fy = f3{C.base_y[0], C.base_y[1], C.base_y[2]};
+    f3 const Fz = f3{C.base_z[0], C.base_z[1], C.base_z[2]};
+    f3 const P = f3{C.pos[0], C.pos[1], C.pos[2]};
+    float const cu = -0.5f * C.w + C.delta * u;
+    float const cv = -0.5f * C.h + C.delta * v;
+    f3 const wij = f3{P.x + Fx.x * cu + Fy.x * cv - C.D * Fz.x, P.y + Fx.y * cu + Fy.y * cv - C.D * Fz.y,
+                      P.z + Fx.z * cu + Fy.z * cv - C.D * Fz.z};
+    float const la = lgpu_flt(&rng) - 0.5f;
+    float const lb = lgpu_flt(&rng) - 0.5f;
+    float const dd = 2.f * C.dof;
+    f3 const wkl = f3{P.x + dd * (Fx.x * la + Fy.x * lb), P.y + dd * (Fx.y * la + Fy.y * lb),
+                      P.z + dd * (Fx.z * la + Fy.z * lb)};
+    f3 const dir = fnorm(f3{wij.x - wkl.x, wij.y - wkl.y, wij.z - wkl.z});
+    float const hero = S.lambda_inf + omega * lgpu_flt(&rng);
+    w.ray[0 * cap + p] = wkl.x;
+    w.ray[1 * cap + p] = wkl.y;
+    w.ray[2 * cap + p] = wkl.z;
+    w.ray[3 * cap + p] = dir.x;
+    w.ray[4 * cap + p] = dir.y;
+    w.ray[5 * cap + p] = dir.z;
+    w.rng[p] = rng;
+    w.hero[p] = hero;
+    w.depth[p] = 0;
+    w.pix[p] = pix;
+    w.samp[p] = s_local;
+    for (uint32_t kk = 0; kk < k_hero; kk++) {
+      w.beta[kk * cap + p] = 1.f;
+      w.acc[kk * cap + p] = 0.f;
+    }
+    w.q_in[qpos + k] = p;
+    paths++;
+  }
+  TravStats const ts{0u, 0u, 0u, 0u};
+  flush_counters(cnt, 0u, paths, ts, 0u);
+}
+
+// Ended paths: their radiance goes to the (sample, pixel) film entry, their
+// slot back to the free list.
+template <int K>
+__global__ void __launch_bounds__(256) wf_finish(DevScene S, WaveState w, DevCounters* cnt) {
+  uint32_t const n = w.ctl[2];
+  float const omega = S.lambda_sup - S.lambda_inf;
+  float const step = omega / float(K);
+  float const prob_l = 1.f / omega;
+  uint32_t nonfinite = 0;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    uint32_t const i = base + threadIdx.x;
+    bool const live = i < n;
+    uint32_t p = 0;
+    if (live) {
+      p = w.fin_list[i];
+      float const hero = w.hero[p];
+      float sx = 0.f, sy = 0.f, sz = 0.f;
+      bool finite = true;
+      for (int k = 0; k < K; k++) {
+        float const val = w.acc[k * w.cap + p] / prob_l;
+        finite = finite && isfinite(val);
+        splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
+      }
+      nonfinite += finite ? 0u : 1u;
+      size_t const o = 3 * (size_t(w.samp[p]) * w.npix + w.pix[p]);
+      w.sbuf[o] = sx;
+      w.sbuf[o + 1] = sy;
+      w.sbuf[o + 2] = sz;
+    }
+    uint32_t const slot = warp_append(&w.ctl[0], live);
+    if (live) w.free_list[slot] = p;
+  }
+  TravStats const ts{0u, 0u, 0u, 0u};
+  flush_counters(cnt, 0u, 0u, ts, nonfinite);
+}
+
+// Film: per pixel, the (sample, pixel) entries summed in sample order.
+__global__ void __launch_bounds__(256) wf_reduce(WaveState w, uint32_t n_samples) {
+  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < w.npix; pix += gridDim.x * blockDim.x) {
+    float X = w.film[3 * pix], Y = w.film[3 * pix + 1], Z = w.film[3 * pix + 2];
+    for (uint32_t s = 0; s < n_samples; s++) {
+      size_t const o = 3 * (size_t(s) * w.npix + pix);
+      X += w.sbuf[o];
+      Y += w.sbuf[o + 1];
+      Z += w.sbuf[o + 2];
+    }
+    w.film[3 * pix] = X;
+    w.film[3 * pix + 1] = Y;
+    w.film[3 * pix + 2] = Z;
+  }
+}
+
 // Persistent instance-BVH traversal of the extension rays (ANY = false,
 // queue q_in, hit records out) or the shadow rays (ANY = true, shadow
 // queue, unoccluded contributions added to the path radiance).  A lane that
@@ -399,7 +538,12 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
         }
       }
     }
-    // compacted appends: next-bounce queue and shadow queue
+    // compacted appends: next-bounce queue, ended paths and shadow queue
+    if (w.fin_list) {
+      bool const ended = live && !cont;
+      uint32_t const fo = warp_append(&w.ctl[2], ended);
+      if (ended) w.fin_list[fo] = p;
+    }
     uint32_t const qo = warp_append(w.n_out, cont);
     if (cont) {
       w.q_out[qo] = p;
