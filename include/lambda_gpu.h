@@ -49,7 +49,9 @@ typedef enum lgpu_status {
   LGPU_ERR_DEVICE_CHECK = -6,
   /* a bounded device-side wait ran out before its condition held */
   LGPU_ERR_TIMEOUT = -7,
-  LGPU_ERR_NO_DEVICE = -8
+  LGPU_ERR_NO_DEVICE = -8,
+  /* a size is beyond an entry point's stated maximum */
+  LGPU_ERR_TOO_LARGE = -9
 } lgpu_status;
 
 /* ---- scene description ------------------------------------------------ */
@@ -259,6 +261,29 @@ int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h,
                  float y_mid, float* out_tonemapped, uint8_t* out_rgb24);
 
 int lgpu_get_stats(const lgpu_ctx* ctx, lgpu_stats* out);
+
+/* Tone map without any device allocation (no counterpart in the reference;
+   it is lgpu_tonemap for callers that cannot allocate device memory at call
+   time, e.g. an engine that owns all device memory in pre-sized pools and
+   must not let a cudaMalloc/cudaFree synchronise the device in its frame
+   loop).  No context is needed.  The caller passes device (or device-
+   accessible) buffers: d_linrgb w*h*3 floats in, d_out_tonemapped w*h*3
+   floats and/or d_out_rgb24 w*h*3 bytes out (either may be NULL), and a
+   stream (NULL: the legacy default stream); the call returns when the
+   results are written.
+   Scratch: the reduction's per-block partial sums and the exposure live in
+   one file-scope __device__ array of LGPU_NOALLOC_SCRATCH_BYTES bytes that
+   every GPU loading the library holds until exit.  Calls share it: two calls
+   that overlap on the same GPU race and must be serialised by the caller.
+   Every slot a call reads is written by that call first, so nothing needs
+   clearing between calls.  The first call on each device looks up the
+   array's device address (cudaGetSymbolAddress) with that device current;
+   make that first call before any stream capture.
+   Limit: w*h <= LGPU_NOALLOC_MAX_PIXELS, else LGPU_ERR_TOO_LARGE. */
+#define LGPU_NOALLOC_MAX_PIXELS (1ull << 31)
+#define LGPU_NOALLOC_SCRATCH_BYTES 9728
+int lgpu_tonemap_noalloc(const float* d_linrgb, uint64_t w, uint64_t h, float y_mid,
+                         float* d_out_tonemapped, uint8_t* d_out_rgb24, void* stream);
 
 /* Host utility for hosts without the reference's builder: builds the wide
    BVH of one mesh exactly as bvh::build does (cg.hpp:632-749), in the

@@ -24,6 +24,7 @@ ERR_UNSUPPORTED = -5
 ERR_DEVICE_CHECK = -6
 ERR_TIMEOUT = -7
 ERR_NO_DEVICE = -8
+ERR_TOO_LARGE = -9
 
 OBJ_SPHERE, OBJ_PLANE, OBJ_TRIMESH = 0, 1, 2
 MAT_LAMBERTIAN, MAT_BLINN, MAT_THINFILM, MAT_MICROFACET, MAT_EMITTER, MAT_DIREMITTER = range(6)
@@ -125,6 +126,8 @@ SIGNATURES = {
     "lgpu_tonemap": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                     _vp, _vp]),
     "lgpu_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),
+    "lgpu_tonemap_noalloc": (ctypes.c_int, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
+                                            _vp, _vp, _vp]),
     "lgpu_build_bvh": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
                                       _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
 }
