@@ -129,16 +129,65 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profile_traffic_per_path():
-    """DRAM bytes per path of the render kernel from the committed ncu
-    summary (profiles/render_instanced_small.json), or None."""
-    p = os.path.join(REPO, "profiles", "render_instanced_small.json")
+def profile_traffic_per_launch(kind):
+    """DRAM bytes (read + write) per launch of kernel kind (0 closest-hit,
+    1 shadow, 2 shading) on the full workload, from the committed ncu
+    summary profiles/traffic_instanced.json, or None."""
+    p = os.path.join(REPO, "profiles", "traffic_instanced.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return float(d["dram_bytes_per_path"])
-    except (OSError, KeyError, ValueError):
+        return float(d["dram_bytes_per_launch"][str(kind)])
+    except (OSError, KeyError, ValueError, TypeError):
         return None
+
+
+KERNEL_NAMES = ("closest-hit traversal (wf_trace_persistent<false> + wf_trace_fallback)",
+                "shadow traversal (wf_trace_persistent<true>)", "shading (wf_shade)")
+
+
+def kernel_roofline(ctx, spp, B, p, stream):
+    """Roofline of the dominant kernel from one untimed render with
+    per-kernel timing (CUDA events around every traversal and shading
+    launch on the render stream, separate work counters per kind).
+    achieved = algorithmic bytes of its launches / their summed device
+    time; the algorithmic bytes are its node, triangle, instance and ray
+    counts times BYTES_PER_*."""
+    import torch
+
+    from lambda_b200 import _lib as L
+    W, H = ctx.size
+    d_out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
+    ctx.render_device(spp, B, p, d_out.data_ptr(), seed=77, flags=L.FLAG_KERNEL_TIMING,
+                      stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    ks = ctx.stats()["kernels"]
+    top = max(range(3), key=lambda k: ks[k]["ms"])
+    k = ks[top]
+    total_ms = sum(x["ms"] for x in ks)
+    peak, peak_kind = measured_peak_hbm()
+    if top == 2 or k["ms"] <= 0:
+        algo = None
+        achieved = None
+    else:
+        algo = (k["node_tests"] * BYTES_PER_NODE + k["tri_tests"] * BYTES_PER_TRI +
+                k["inst_tests"] * BYTES_PER_INST + k["rays"] * BYTES_PER_RAY)
+        achieved = algo / (k["ms"] / 1e3) / 1e9
+    launches = max(int(k["launches"]), 1)
+    tpl = profile_traffic_per_launch(top)
+    return {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": (achieved / peak) if achieved is not None else None,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else peak_kind,
+            "traffic": tpl,
+            "algorithmic_bytes_per_launch": (algo / launches) if algo is not None else None,
+            "avg_launch_ms": k["ms"] / launches, "launches": int(k["launches"]),
+            "share_of_kernel_time": k["ms"] / total_ms if total_ms > 0 else None,
+            "per_launch": {"rays": k["rays"] / launches, "node_tests": k["node_tests"] / launches,
+                           "tri_tests": k["tri_tests"] / launches,
+                           "inst_tests": k["inst_tests"] / launches},
+            "mrays_per_s": k["rays"] / (k["ms"] / 1e3) / 1e6 if k["ms"] > 0 else None,
+            "kernels_ms": {KERNEL_NAMES[i].split(" (")[0]: ks[i]["ms"] for i in range(3)}}
 
 
 def cpu_reference_sample(nls, w, budget_s, fast=True):
@@ -284,20 +333,8 @@ def run_device(args, w):
                    "readback) per step"}
 
     c = counters[-1]
-    algo = (c["node_tests"] * BYTES_PER_NODE + c["tri_tests"] * BYTES_PER_TRI +
-            c["inst_tests"] * BYTES_PER_INST + c["rays"] * BYTES_PER_RAY)
-    avg_kernel_s = statistics.mean(kern_ms) / 1e3
-    peak, peak_kind = measured_peak_hbm()
-    achieved = algo / avg_kernel_s / 1e9
-    tpp = profile_traffic_per_path()
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": (tpp * paths_per_step) if tpp is not None else None,
-                "algorithmic_bytes_per_launch": int(algo),
-                "per_launch": {"paths": int(c["paths"]), "rays": int(c["rays"]),
-                               "node_tests": int(c["node_tests"]), "tri_tests": int(c["tri_tests"]),
-                               "inst_tests": int(c["inst_tests"])},
-                "mrays_per_s": c["rays"] / avg_kernel_s / 1e6}
+    launches_per_step = int(c["launches"])
+    roofline = kernel_roofline(ctx, spp, B, p, stream)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -306,7 +343,8 @@ def run_device(args, w):
             "config": {"workload": workload_desc(w), "paths_per_step_per_gpu": paths_per_step,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": "frame per GPU" if world > 1 else "single GPU"},
-            "e2e": e2e, "roofline": roofline, "clocks": clk, "gpu_launches": args.steps,
+            "e2e": e2e, "roofline": roofline, "clocks": clk,
+            "gpu_launches": launches_per_step * args.steps,
             "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
     if rank == 0 and world == 1 and not args.no_baseline:
         from oracle import refharness

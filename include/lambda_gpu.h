@@ -191,6 +191,11 @@ typedef struct lgpu_scene {
    the same random numbers per path. */
 #define LGPU_FLAG_MEGAKERNEL 0x2u
 
+/* Time the wavefront's closest-hit, shadow and shading launches separately
+   (CUDA events around each launch) and count their traversal work apart;
+   results in lgpu_stats.kernel_*.  For profiling; it adds event records. */
+#define LGPU_FLAG_KERNEL_TIMING 0x4u
+
 /* Renderer settings (include/renderer.hpp:35-37) plus the device RNG seed. */
 typedef struct lgpu_render_params {
   uint32_t spp;             /* Renderer::SPP */
@@ -221,11 +226,20 @@ typedef struct lgpu_stats {
   uint32_t device_checks;   /* device-side checks that fired */
   uint32_t max_stack;       /* traversal stack bound in use */
   uint32_t nonfinite_paths; /* paths whose radiance was NaN or infinite */
-  uint32_t reserved;
+  uint32_t launches;        /* kernel launches of the last render or trace */
   uint64_t node_tests; /* 8-wide node box tests of the last kernel */
   uint64_t tri_tests;  /* triangle tests */
   uint64_t inst_tests; /* object (instance) tests */
   uint64_t upload_bytes; /* host-to-device bytes of the last scene upload */
+  /* with LGPU_FLAG_KERNEL_TIMING: [0] closest-hit traversal, [1] shadow
+     traversal, [2] shading — summed device time, launches, rays, node,
+     triangle and instance tests of each kind */
+  double kernel_ms[3];
+  uint64_t kernel_launches[3];
+  uint64_t kernel_rays[3];
+  uint64_t kernel_node_tests[3];
+  uint64_t kernel_tri_tests[3];
+  uint64_t kernel_inst_tests[3];
 } lgpu_stats;
 
 /* Context.  `device` is a CUDA ordinal. */

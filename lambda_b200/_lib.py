@@ -107,9 +107,15 @@ class Stats(ctypes.Structure):
     _fields_ = [("last_kernel_ms", ctypes.c_double), ("rays", ctypes.c_uint64),
                 ("paths", ctypes.c_uint64), ("device_checks", ctypes.c_uint32),
                 ("max_stack", ctypes.c_uint32), ("nonfinite_paths", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32), ("node_tests", ctypes.c_uint64),
+                ("launches", ctypes.c_uint32), ("node_tests", ctypes.c_uint64),
                 ("tri_tests", ctypes.c_uint64), ("inst_tests", ctypes.c_uint64),
-                ("upload_bytes", ctypes.c_uint64)]
+                ("upload_bytes", ctypes.c_uint64), ("kernel_ms", ctypes.c_double * 3),
+                ("kernel_launches", ctypes.c_uint64 * 3), ("kernel_rays", ctypes.c_uint64 * 3),
+                ("kernel_node_tests", ctypes.c_uint64 * 3), ("kernel_tri_tests", ctypes.c_uint64 * 3),
+                ("kernel_inst_tests", ctypes.c_uint64 * 3)]
+
+FLAG_KERNEL_TIMING = 0x4
+KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2
 
 
 # every entry point of include/lambda_gpu.h: name -> (restype, argtypes)

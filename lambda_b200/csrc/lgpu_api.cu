@@ -61,8 +61,10 @@ struct lgpu_ctx {
   DevArray<double> partials;
   DevArray<float> tm_in, tm_out;
   DevArray<uint8_t> tm_24;
-  DevCounters* counters = nullptr;
+  DevCounters* counters = nullptr;  // 3 records: all kernels, closest-hit, shadow
   float* exposure = nullptr;
+  KernelTimer timer;
+  bool timer_ready = false;
 
   void release_scene() {
     objects.release();
@@ -119,13 +121,23 @@ int bind_device(lgpu_ctx* ctx) {
 
 // Reads the device counters after a launch, updates the stats and reports
 // device-side checks.
-int collect(lgpu_ctx* ctx, const char* what) {
-  DevCounters c;
-  cudaError_t e = cudaMemcpyAsync(&c, ctx->counters, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream);
+int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
+  DevCounters r[3];
+  cudaError_t e = cudaMemcpyAsync(r, ctx->counters, sizeof(r), cudaMemcpyDeviceToHost, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, what);
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess) ctx->stats.last_kernel_ms = ms;
+  DevCounters c = r[0];
+  for (int k = 1; k < 3; k++) {
+    c.rays += r[k].rays;
+    c.paths += r[k].paths;
+    c.nodes += r[k].nodes;
+    c.tris += r[k].tris;
+    c.insts += r[k].insts;
+    c.flags |= r[k].flags;
+    c.nonfinite += r[k].nonfinite;
+  }
   ctx->stats.rays = c.rays;
   ctx->stats.paths = c.paths;
   ctx->stats.device_checks = c.flags;
@@ -133,6 +145,18 @@ int collect(lgpu_ctx* ctx, const char* what) {
   ctx->stats.tri_tests = c.tris;
   ctx->stats.inst_tests = c.insts;
   ctx->stats.nonfinite_paths = c.nonfinite;
+  ctx->stats.launches = uint32_t(ctx->timer.total);
+  for (int k = 0; k < 3; k++) {
+    ctx->stats.kernel_ms[k] = timed ? ctx->timer.ms[k] : 0.0;
+    ctx->stats.kernel_launches[k] = timed ? ctx->timer.launches[k] : 0;
+    // counters: [1] closest-hit, [2] shadow; shading does no traversal
+    DevCounters const z{};
+    const DevCounters& s = (timed && k < 2) ? r[k + 1] : z;
+    ctx->stats.kernel_rays[k] = s.rays;
+    ctx->stats.kernel_node_tests[k] = s.nodes;
+    ctx->stats.kernel_tri_tests[k] = s.tris;
+    ctx->stats.kernel_inst_tests[k] = s.insts;
+  }
   if (c.flags & 1u)
     return fail(ctx, LGPU_ERR_DEVICE_CHECK,
                 std::string(what) + ": a traversal stack bound was exceeded; results are incomplete");
@@ -231,12 +255,27 @@ int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaSt
     if (r != LGPU_OK) return r;
     wave = &ws;
   }
-  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), st);
+  bool const timing = (p->flags & LGPU_FLAG_KERNEL_TIMING) && wave;
+  if (timing && !ctx->timer_ready) {
+    for (auto& k : ctx->timer.ev)
+      for (auto& s : k)
+        for (cudaEvent_t& ev : s)
+          if (!ev && cudaEventCreate(&ev) != cudaSuccess) return fail(ctx, LGPU_ERR_CUDA, "timing events");
+    ctx->timer_ready = true;
+  }
+  ctx->timer.reset(timing);
+  KernelTimer* const timer = &ctx->timer;
+  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  if (e == cudaSuccess) e = launch_render(ctx->S, a, wave, d_out, ctx->counters, st);
+  if (e == cudaSuccess) e = launch_render(ctx->S, a, wave, d_out, ctx->counters, st, timer);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return LGPU_OK;
+}
+
+// per-kernel timing applies to the wavefront kernels only
+bool timing_requested(const lgpu_render_params* p) {
+  return (p->flags & LGPU_FLAG_KERNEL_TIMING) && !(p->flags & LGPU_FLAG_MEGAKERNEL);
 }
 
 }  // namespace
@@ -258,7 +297,7 @@ int lgpu_create(int device, lgpu_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, sizeof(DevCounters));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, 3 * sizeof(DevCounters));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->exposure, sizeof(float));
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, 8 * sizeof(uint32_t));
   if (e != cudaSuccess) {
@@ -295,6 +334,10 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->exposure) cudaFree(ctx->exposure);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (auto& k : ctx->timer.ev)
+    for (auto& s : k)
+      for (cudaEvent_t ev : s)
+        if (ev) cudaEventDestroy(ev);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -374,7 +417,7 @@ int lgpu_render_device(lgpu_ctx* ctx, const lgpu_render_params* params, float* d
     cudaError_t const e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
   }
-  return collect(ctx, "render");
+  return collect(ctx, "render", timing_requested(params));
 }
 
 int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linrgb) {
@@ -388,7 +431,7 @@ int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linr
   if (rc != LGPU_OK) return rc;
   e = cudaMemcpyAsync(out_linrgb, ctx->out.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render readback");
-  return collect(ctx, "render");
+  return collect(ctx, "render", timing_requested(params));
 }
 
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {
@@ -401,8 +444,10 @@ int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t fl
   if (e != cudaSuccess) return cuda_fail(ctx, e, "ray buffers");
   cudaStream_t const st = ctx->stream;
   e = cudaMemcpyAsync(ctx->rays.ptr, rays, 6 * n * sizeof(float), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
+  ctx->timer.reset(false);
+  ctx->timer.total = 1;
   if (e == cudaSuccess) e = launch_trace(ctx->S, ctx->rays.ptr, n, flags, ctx->hits.ptr, ctx->counters, st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e == cudaSuccess)

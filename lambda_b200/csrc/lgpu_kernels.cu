@@ -130,12 +130,12 @@ cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uin
 }
 
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                          DevCounters* d_cnt, cudaStream_t st) {
+                          DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
   if (a.pixel_count == 0) return cudaSuccess;
   switch (S.hero_k) {
-    case 4: return launch_render_k<4>(S, a, wave, d_out, d_cnt, st);
-    case 8: return launch_render_k<8>(S, a, wave, d_out, d_cnt, st);
-    case 16: return launch_render_k<16>(S, a, wave, d_out, d_cnt, st);
+    case 4: return launch_render_k<4>(S, a, wave, d_out, d_cnt, st, timer);
+    case 8: return launch_render_k<8>(S, a, wave, d_out, d_cnt, st, timer);
+    case 16: return launch_render_k<16>(S, a, wave, d_out, d_cnt, st, timer);
   }
   return cudaErrorInvalidValue;
 }

@@ -71,13 +71,58 @@ struct RenderArgs {
 cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
                          lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st);
 
-cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                          DevCounters* d_cnt, cudaStream_t st);
+// Launch bookkeeping of one render: the number of kernel launches, and
+// with `on` the device time of the wavefront's launches per kind (0
+// closest-hit traversal, 1 shadow traversal, 2 shading), from pairs of
+// events recorded around each launch and read back after the stream
+// synchronises.
+struct KernelTimer {
+  static constexpr int kSlots = 16;
+  bool on = false;
+  unsigned long long total = 0;  // kernel launches
+  cudaEvent_t ev[3][kSlots][2] = {};
+  int used[3] = {0, 0, 0};
+  double ms[3] = {0, 0, 0};
+  unsigned long long launches[3] = {0, 0, 0};
+  void reset(bool timing) {
+    on = timing;
+    total = 0;
+    for (int k = 0; k < 3; k++) {
+      used[k] = 0;
+      ms[k] = 0.0;
+      launches[k] = 0;
+    }
+  }
+  void begin(int k, cudaStream_t st) {
+    if (on) cudaEventRecord(ev[k][used[k]][0], st);
+  }
+  void end(int k, cudaStream_t st) {
+    if (!on) return;
+    cudaEventRecord(ev[k][used[k]][1], st);
+    used[k]++;
+    launches[k]++;
+  }
+  // after the stream has synchronised
+  void harvest() {
+    if (!on) return;
+    for (int k = 0; k < 3; k++) {
+      for (int i = 0; i < used[k]; i++) {
+        float m = 0.f;
+        if (cudaEventElapsedTime(&m, ev[k][i][0], ev[k][i][1]) == cudaSuccess) ms[k] += m;
+      }
+      used[k] = 0;
+    }
+  }
+};
+
 // Renders with the wavefront kernels when wave != nullptr, else with the
-// one-thread-per-pixel megakernel.
+// one-thread-per-pixel megakernel.  d_cnt points at 3 counter records:
+// everything, and with timer->on the closest-hit and shadow traversal apart.
 template <int K>
 cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                            DevCounters* d_cnt, cudaStream_t st);
+                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
+                          DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
 
 // Samples per pixel in one wave for a frame of npix pixels: enough paths in
 // flight to fill the GPU (about 2^21), never more than spp.

@@ -97,10 +97,13 @@ uint32_t persistent_blocks(F kernel, int threads, size_t smem) {
 
 template <int K>
 cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                            DevCounters* d_cnt, cudaStream_t st) {
+                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+  DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
+  DevCounters* const c_shadow = timer->on ? d_cnt + 2 : d_cnt;
   if (!wave) {
     uint32_t const blocks = (a.pixel_count + 127) / 128;
     render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
+    timer->total++;
     return cudaGetLastError();
   }
   WaveState w = *wave;
@@ -135,6 +138,7 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
     uint32_t const ns = (a.spp - s0 < chunk) ? (a.spp - s0) : chunk;
     uint32_t const total = ns * w.npix;
     wf_stream_init<<<g_gen, 256, 0, st>>>(w);
+    timer->total++;
     for (uint32_t it = 0;; it++) {
       wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
       cudaMemsetAsync(w.ctl + 2, 0, sizeof(uint32_t), st);
@@ -142,15 +146,23 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
       wf_generate_stream<<<g_gen, 256, 0, st>>>(S, a, w, K, s0, d_cnt);
       cudaMemsetAsync(w.n_out, 0, sizeof(uint32_t), st);
       cudaMemsetAsync(w.n_shadow, 0, 4 * sizeof(uint32_t), st);  // n_shadow, fetch[2], n_fb
+      timer->begin(0, st);
       if (linear) {
-        wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, d_cnt);
+        wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, c_closest);
       } else {
-        wf_trace_persistent<false, K><<<g_ptrace, 128, smem, st>>>(S, w, d_cnt);
-        wf_trace_fallback<<<g_fb, 128, 0, st>>>(S, w, d_cnt);
+        wf_trace_persistent<false, K><<<g_ptrace, 128, smem, st>>>(S, w, c_closest);
+        wf_trace_fallback<<<g_fb, 128, 0, st>>>(S, w, c_closest);
       }
+      timer->end(0, st);
+      timer->begin(2, st);
       wf_shade<K><<<g_shade, 128, 0, st>>>(S, a, w, d_cnt);
-      if (linear) wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, d_cnt);
-      else wf_trace_persistent<true, K><<<g_pshadow, 128, smem, st>>>(S, w, d_cnt);
+      timer->end(2, st);
+      timer->begin(1, st);
+      if (linear) wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, c_shadow);
+      else wf_trace_persistent<true, K><<<g_pshadow, 128, smem, st>>>(S, w, c_shadow);
+      timer->end(1, st);
+      // finish, plan, generate, trace (+ fallback), shade, shadow
+      timer->total += linear ? 6 : 7;
       uint32_t* t = w.q_in;
       w.q_in = w.q_out;
       w.q_out = t;
@@ -164,16 +176,23 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
         cudaMemcpyAsync(w.h_ctl + 3, w.n_in, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) break;
+        timer->harvest();
         if (w.h_ctl[1] == total && w.h_ctl[3] == 0) break;
       }
     }
     if (e != cudaSuccess) break;
     wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
     wf_reduce<<<(w.npix + 255) / 256, 256, 0, st>>>(w, ns);
+    timer->total += 2;
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = launch_finalize(w.film, w.npix, uint32_t(S.cam.width), uint32_t(S.cam.height),
                                             float(a.spp) * float(K), S.lambda_delta, d_out, st);
+  timer->total++;
+  if (timer->on && e == cudaSuccess) {
+    e = cudaStreamSynchronize(st);
+    timer->harvest();
+  }
   return e;
 }
 

@@ -109,7 +109,11 @@ class Context:
                 "device_checks": s.device_checks, "max_stack": s.max_stack,
                 "nonfinite_paths": s.nonfinite_paths, "node_tests": s.node_tests,
                 "tri_tests": s.tri_tests, "inst_tests": s.inst_tests,
-                "upload_bytes": s.upload_bytes}
+                "upload_bytes": s.upload_bytes, "launches": s.launches,
+                "kernels": [{"ms": s.kernel_ms[k], "launches": s.kernel_launches[k],
+                             "rays": s.kernel_rays[k], "node_tests": s.kernel_node_tests[k],
+                             "tri_tests": s.kernel_tri_tests[k],
+                             "inst_tests": s.kernel_inst_tests[k]} for k in range(3)]}
 
 
 def hits_to_numpy(arr, n):

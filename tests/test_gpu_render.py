@@ -76,3 +76,30 @@ def test_tonemap_matches_reference(small_mixed):
     # in double: tone-mapped values agree to 1e-4 relative, bytes within 1
     assert np.allclose(tm_g, tm_r, rtol=1e-4, atol=1e-6)
     assert np.max(np.abs(b_g.astype(int) - b_r.astype(int))) <= 1
+
+
+@pytest.mark.parametrize("n_inst", [2, 12])
+def test_kernel_timing_changes_nothing(scene_dir, n_inst):
+    """FLAG_KERNEL_TIMING only adds event records and splits the work
+    counters per kernel kind: the image is bit-identical and the per-kind
+    counters add up to the totals."""
+    import os
+    from lambda_b200 import synth
+    nls = synth.instanced(os.path.join(str(scene_dir), "inst_timing_%d" % n_inst),
+                          n_instances=n_inst, subdiv=3, width=64)
+    ctx = Context()
+    ctx.upload(load_nls(nls))
+    a = ctx.render(8, 8, 0.8, seed=3)
+    s0 = ctx.stats()
+    b = ctx.render(8, 8, 0.8, seed=3, flags=L.FLAG_KERNEL_TIMING)
+    s1 = ctx.stats()
+    assert np.array_equal(a, b)
+    assert s0["rays"] == s1["rays"] and s0["node_tests"] == s1["node_tests"]
+    assert s0["launches"] == s1["launches"] > 0
+    ks = s1["kernels"]
+    assert ks[0]["rays"] + ks[1]["rays"] == s1["rays"]
+    assert ks[0]["node_tests"] + ks[1]["node_tests"] == s1["node_tests"]
+    assert ks[0]["tri_tests"] + ks[1]["tri_tests"] == s1["tri_tests"]
+    assert all(k["launches"] == ks[0]["launches"] > 0 for k in ks)
+    assert all(k["ms"] > 0 for k in ks)
+    assert all(k["ms"] == 0 for k in s0["kernels"])
