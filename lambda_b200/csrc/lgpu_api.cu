@@ -48,14 +48,9 @@ struct lgpu_ctx {
   DevArray<float> cmf;
   // working buffers
   DevArray<float> out;
-  // wavefront state (lgpu_wave.cuh), sized for the last frame rendered
-  DevArray<float> w_ray, w_hero, w_beta, w_acc, w_hit, w_sray, w_scontrib, w_film;
-  DevArray<uint64_t> w_rng;
-  DevArray<uint32_t> w_depth, w_q0, w_q1, w_spath, w_counts, w_fb;
-  DevArray<uint32_t> w_pix, w_samp, w_free, w_fin, w_ctl;
-  DevArray<float> w_sbuf;
+  // wavefront state (lgpu_wave.cuh), sized for the largest frame rendered
+  DevArray<uint8_t> w_arena;
   uint32_t* h_ctl = nullptr;  // pinned
-  uint32_t w_cap = 0, w_k = 0, w_npix = 0, w_chunk = 0;
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
   DevArray<double> partials;
@@ -163,6 +158,47 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
   return LGPU_OK;
 }
 
+// Carves 256-byte aligned pieces out of one device allocation.
+struct Carver {
+  uint8_t* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t n) {
+    T* const p = reinterpret_cast<T*>(base ? base + off : nullptr);
+    off += (n * sizeof(T) + 255) & ~size_t(255);
+    return p;
+  }
+};
+
+// Lays out the wavefront buffers for queue capacity cap, K hero
+// wavelengths, npix pixels and ns samples per chunk; with base == nullptr
+// it only counts the bytes.
+size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint32_t ns, WaveState& ws) {
+  Carver c{base};
+  size_t const n = cap;
+  for (PathBuf* pb : {&ws.in, &ws.out}) {
+    pb->ray = c.take<float>(6 * n);
+    pb->rng = c.take<uint64_t>(n);
+    pb->hero = c.take<float>(n);
+    pb->depth = c.take<uint32_t>(n);
+    pb->item = c.take<uint32_t>(n);
+    pb->beta = c.take<float>(size_t(K) * n);
+    pb->acc = c.take<float>(size_t(K) * n);
+  }
+  ws.hit = c.take<float>(9 * n);
+  ws.e_acc = c.take<float>(size_t(K) * n);
+  ws.e_hero = c.take<float>(n);
+  ws.e_item = c.take<uint32_t>(n);
+  ws.sray = c.take<float>(8 * n);
+  ws.s_target = c.take<uint32_t>(n);
+  ws.s_contrib = c.take<float>(size_t(K) * n);
+  ws.fb_queue = c.take<uint32_t>(n);
+  ws.ctl = c.take<uint32_t>(kCtlWords);
+  ws.film = c.take<float>(3 * size_t(npix));
+  ws.sbuf = c.take<float>(3 * size_t(npix) * ns);
+  return c.off;
+}
+
 // Sizes the wavefront buffers for a frame of npix pixels and fills ws.
 int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
   uint32_t const K = ctx->S.hero_k;
@@ -172,67 +208,16 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
   // samples per chunk: the (sample, pixel) film buffer stays under 2 GiB
   uint64_t const max_ns = (uint64_t(1) << 31) / (12ull * npix);
   uint32_t const ns = uint32_t(spp < max_ns ? spp : (max_ns ? max_ns : 1));
-  if (cap != ctx->w_cap || K != ctx->w_k || npix != ctx->w_npix || ns != ctx->w_chunk) {
-    size_t const c = cap;
-    cudaError_t e = ensure(ctx->w_ray, 6 * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_hero, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_beta, size_t(K) * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_acc, size_t(K) * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_hit, 9 * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_sray, 8 * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_scontrib, size_t(K) * c);
-    if (e == cudaSuccess) e = ensure(ctx->w_film, 3 * size_t(npix));
-    if (e == cudaSuccess) e = ensure(ctx->w_rng, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_depth, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_q0, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_q1, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_spath, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_fb, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_counts, 8);
-    if (e == cudaSuccess) e = ensure(ctx->w_pix, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_samp, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_free, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_fin, c);
-    if (e == cudaSuccess) e = ensure(ctx->w_ctl, 8);
-    if (e == cudaSuccess) e = ensure(ctx->w_sbuf, 3 * size_t(npix) * ns);
-    if (e != cudaSuccess) {
-      ctx->w_cap = 0;
-      return cuda_fail(ctx, e, "wavefront buffers");
-    }
-    ctx->w_cap = cap;
-    ctx->w_k = K;
-    ctx->w_npix = npix;
-    ctx->w_chunk = ns;
-  }
+  size_t const bytes = wave_layout(nullptr, cap, K, npix, ns, ws);
+  cudaError_t const e = ensure(ctx->w_arena, bytes);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront buffers");
+  wave_layout(ctx->w_arena.ptr, cap, K, npix, ns, ws);
   ws.cap = cap;
   ws.npix = npix;
   ws.n_samples = ns;
-  ws.pix = ctx->w_pix.ptr;
-  ws.samp = ctx->w_samp.ptr;
-  ws.free_list = ctx->w_free.ptr;
-  ws.fin_list = ctx->w_fin.ptr;
-  ws.ctl = ctx->w_ctl.ptr;
+  ws.n_in = ws.ctl + kCtlCountA;
+  ws.n_out = ws.ctl + kCtlCountB;
   ws.h_ctl = ctx->h_ctl;
-  ws.sbuf = ctx->w_sbuf.ptr;
-  ws.ray = ctx->w_ray.ptr;
-  ws.rng = ctx->w_rng.ptr;
-  ws.hero = ctx->w_hero.ptr;
-  ws.depth = ctx->w_depth.ptr;
-  ws.beta = ctx->w_beta.ptr;
-  ws.acc = ctx->w_acc.ptr;
-  ws.hit = ctx->w_hit.ptr;
-  ws.q_in = ctx->w_q0.ptr;
-  ws.q_out = ctx->w_q1.ptr;
-  ws.n_in = ctx->w_counts.ptr;
-  ws.n_out = ctx->w_counts.ptr + 1;
-  ws.n_shadow = ctx->w_counts.ptr + 2;
-  ws.fetch = ctx->w_counts.ptr + 3;
-  ws.n_fb = ctx->w_counts.ptr + 5;
-  ws.fb_queue = ctx->w_fb.ptr;
-  ws.sray = ctx->w_sray.ptr;
-  ws.s_path = ctx->w_spath.ptr;
-  ws.s_contrib = ctx->w_scontrib.ptr;
-  ws.film = ctx->w_film.ptr;
   return LGPU_OK;
 }
 
@@ -299,7 +284,7 @@ int lgpu_create(int device, lgpu_ctx** out) {
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, 3 * sizeof(DevCounters));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->exposure, sizeof(float));
-  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, 8 * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, kCtlWords * sizeof(uint32_t));
   if (e != cudaSuccess) {
     lgpu_destroy(ctx);
     return e == cudaErrorMemoryAllocation ? LGPU_ERR_OUT_OF_MEMORY : LGPU_ERR_CUDA;
@@ -314,15 +299,7 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   ctx->release_scene();
   ctx->out.release();
-  for (DevArray<float>* a : {&ctx->w_ray, &ctx->w_hero, &ctx->w_beta, &ctx->w_acc, &ctx->w_hit,
-                             &ctx->w_sray, &ctx->w_scontrib, &ctx->w_film})
-    a->release();
-  ctx->w_rng.release();
-  for (DevArray<uint32_t>* a : {&ctx->w_depth, &ctx->w_q0, &ctx->w_q1, &ctx->w_spath, &ctx->w_counts,
-                                &ctx->w_fb, &ctx->w_pix, &ctx->w_samp, &ctx->w_free, &ctx->w_fin,
-                                &ctx->w_ctl})
-    a->release();
-  ctx->w_sbuf.release();
+  ctx->w_arena.release();
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   ctx->rays.release();
   ctx->hits.release();

@@ -18,42 +18,52 @@ struct DevCounters {
   unsigned int nonfinite;    // paths whose radiance was NaN or infinite
 };
 
-// Device buffers of the wavefront renderer (lgpu_wave.cuh), per-path state
-// in structure-of-arrays layout; the context owns them.
+// Path state of one queue of the wavefront renderer (lgpu_wave.cuh): path
+// i of the queue at index i of every field, field-major.
+struct PathBuf {
+  float* ray;       // 6*cap (ox, oy, oz, dx, dy, dz)
+  uint64_t* rng;    // cap
+  float* hero;      // cap
+  uint32_t* depth;  // cap
+  uint32_t* item;   // cap: work item (sample * npix + pixel, relative to the chunk)
+  float* beta;      // K*cap
+  float* acc;       // K*cap
+};
+
+// Counters of the wavefront renderer (WaveState::ctl).
+constexpr int kCtlCountA = 0;    // queue lengths of the two PathBufs
+constexpr int kCtlCountB = 1;
+constexpr int kCtlShadow = 2;    // shadow rays
+constexpr int kCtlFetch = 3;     // 2 work counters of the persistent trace kernels
+constexpr int kCtlFallback = 5;  // rays re-traced in the reference's object order
+constexpr int kCtlEnded = 6;     // ended paths
+constexpr int kCtlNext = 7;      // next work item to start
+constexpr int kCtlNew = 8;       // plan of the next generate: new paths,
+constexpr int kCtlFirst = 9;     //   their first work item,
+constexpr int kCtlPos = 10;      //   their first queue position
+constexpr int kCtlWords = 16;
+constexpr uint32_t kEndedBit = 0x80000000u;
+
+// Device buffers of the wavefront renderer; the context owns them.
 struct WaveState {
-  uint32_t cap;      // path slots
-  uint32_t npix;     // pixels of the frame
-  uint32_t n_samples;  // samples per pixel in this wave (cap >= npix*n_samples)
-  float* ray;        // 6*cap (ox, oy, oz, dx, dy, dz), field-major
-  uint64_t* rng;     // cap
-  float* hero;       // cap
-  uint32_t* depth;   // cap
-  float* beta;       // K*cap
-  float* acc;        // K*cap
-  float* hit;        // 9*cap (z, obj, face, b0, b1, b2, plx, ply, plz)
-  uint32_t* q_in;    // active path slots
-  uint32_t* q_out;
-  uint32_t* n_in;    // device counts
+  uint32_t cap;        // queue capacity (paths in flight)
+  uint32_t npix;       // pixels of the frame
+  uint32_t n_samples;  // samples per pixel in one chunk of the frame
+  PathBuf in, out;     // current and next queue, swapped every iteration
+  uint32_t* n_in;      // queue lengths (in ctl), swapped with the queues
   uint32_t* n_out;
-  float* sray;       // 8*cap (ox, oy, oz, dx, dy, dz, tmax, skip)
-  uint32_t* s_path;  // cap
-  float* s_contrib;  // K*cap
-  uint32_t* n_shadow;
-  uint32_t* fetch;     // 2 work counters of the persistent trace kernels
-  uint32_t* fb_queue;  // extension rays re-traced in the reference's object order
-  uint32_t* n_fb;
-  // streaming: a slot whose path ends is refilled with the next
-  // (sample, pixel) of the frame
-  uint32_t* pix;        // cap: pixel of the slot's path
-  uint32_t* samp;       // cap: sample index (relative to the chunk)
-  uint32_t* free_list;  // cap
-  uint32_t* fin_list;   // cap: slots whose path ended this iteration
-  uint32_t* ctl;        // [0] free slots, [1] next work item, [2] ended paths,
-                        // [3..6] plan of the next generate (new, first item,
-                        // free-list top, queue position)
-  uint32_t* h_ctl;      // pinned host copy of ctl[0..2] and the queue count
-  float* sbuf;          // 3 * npix * n_samples: XYZ of every (sample, pixel)
-  float* film;       // 3*npix XYZ
+  float* hit;          // 9*cap closest hits of `in` (z, obj, face, b0, b1, b2, plx, ply, plz)
+  float* e_acc;        // K*cap: radiance of the paths ended this iteration
+  float* e_hero;       // cap
+  uint32_t* e_item;    // cap
+  float* sray;         // 8*cap shadow rays (ox, oy, oz, dx, dy, dz, tmax, skip)
+  uint32_t* s_target;  // cap: path of each shadow ray (`out` index, or ended index | kEndedBit)
+  float* s_contrib;    // K*cap
+  uint32_t* fb_queue;  // cap: `in` indices re-traced in the reference's object order
+  uint32_t* ctl;       // kCtlWords counters
+  uint32_t* h_ctl;     // pinned host copy of ctl
+  float* sbuf;         // 3 * npix * n_samples: XYZ of every (sample, pixel)
+  float* film;         // 3*npix XYZ
 };
 
 struct RenderArgs {

@@ -109,7 +109,7 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
   WaveState w = *wave;
   size_t const smem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
   static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0, g_ptrace = 0, g_pshadow = 0,
-                  g_fb = 0;
+                  g_fb = 0, g_fin = 0;
   if (!g_trace) {
     cudaFuncSetAttribute(wf_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(wf_shadow<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -122,30 +122,28 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
     g_ptrace = persistent_blocks(wf_trace_persistent<false, K>, 128, smem);
     g_pshadow = persistent_blocks(wf_trace_persistent<true, K>, 128, smem);
     g_shade = persistent_blocks(wf_shade<K>, 128, 0);
-    g_gen = persistent_blocks(wf_generate, 256, 0);
+    g_gen = persistent_blocks(wf_generate_stream<K>, 256, 0);
+    g_fin = persistent_blocks(wf_finish<K>, 256, 0);
     g_fb = persistent_blocks(wf_trace_fallback, 128, 0);
   }
   // the instance BVH kernels, or the reference's linear object loop
   bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
-  // Streaming: every iteration ends paths (finish), starts new ones in the
-  // freed slots (plan + generate), then advances every path in flight by
-  // one segment (trace, shade, shadow).  The frame's samples are processed
-  // in chunks of w.n_samples (the size of the (sample, pixel) film buffer).
+  // Streaming: every iteration finishes the paths that ended in the last
+  // one, appends new paths behind the queue up to its capacity (plan +
+  // generate), then advances every queued path by one segment (trace,
+  // shade, shadow).  The frame's samples are processed in chunks of
+  // w.n_samples (the size of the (sample, pixel) film buffer).
   uint32_t const chunk = w.n_samples;
-  uint32_t const g_fin = g_gen;
   for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
     uint32_t const ns = (a.spp - s0 < chunk) ? (a.spp - s0) : chunk;
     uint32_t const total = ns * w.npix;
-    wf_stream_init<<<g_gen, 256, 0, st>>>(w);
+    wf_stream_init<<<1, 32, 0, st>>>(w);
     timer->total++;
     for (uint32_t it = 0;; it++) {
       wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
-      cudaMemsetAsync(w.ctl + 2, 0, sizeof(uint32_t), st);
       wf_plan<<<1, 1, 0, st>>>(w, total);
-      wf_generate_stream<<<g_gen, 256, 0, st>>>(S, a, w, K, s0, d_cnt);
-      cudaMemsetAsync(w.n_out, 0, sizeof(uint32_t), st);
-      cudaMemsetAsync(w.n_shadow, 0, 4 * sizeof(uint32_t), st);  // n_shadow, fetch[2], n_fb
+      wf_generate_stream<K><<<g_gen, 256, 0, st>>>(S, a, w, s0, d_cnt);
       timer->begin(0, st);
       if (linear) {
         wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, c_closest);
@@ -163,21 +161,21 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
       timer->end(1, st);
       // finish, plan, generate, trace (+ fallback), shade, shadow
       timer->total += linear ? 6 : 7;
-      uint32_t* t = w.q_in;
-      w.q_in = w.q_out;
-      w.q_out = t;
-      t = w.n_in;
+      PathBuf const pb = w.in;
+      w.in = w.out;
+      w.out = pb;
+      uint32_t* const pc = w.n_in;
       w.n_in = w.n_out;
-      w.n_out = t;
+      w.n_out = pc;
       // look at the counters every few iterations: done when every work
-      // item was started and no path is in flight
+      // item was started and the queue is empty
       if ((it & 3) == 3) {
-        cudaMemcpyAsync(w.h_ctl, w.ctl, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(w.h_ctl + 3, w.n_in, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(w.h_ctl, w.ctl, kCtlWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) break;
         timer->harvest();
-        if (w.h_ctl[1] == total && w.h_ctl[3] == 0) break;
+        uint32_t const n_in = w.h_ctl[w.n_in - w.ctl];
+        if (w.h_ctl[kCtlNext] == total && n_in == 0) break;
       }
     }
     if (e != cudaSuccess) break;

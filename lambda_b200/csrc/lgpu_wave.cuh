@@ -1,25 +1,31 @@
-// lgpu_wave.cuh — wavefront path tracing.
+// lgpu_wave.cuh — streaming wavefront path tracing.
 //
-// A wave is a set of paths (n_samples samples of every pixel) processed one
-// bounce at a time by short kernels over compacted queues:
+// Paths in flight live in queue order: path i of the current queue keeps
+// its state at index i of the `in` buffers (field-major, so a warp's access
+// to one field is one coalesced transaction).  Each iteration
 //
-//   wf_generate   camera ray + hero wavelengths of every path of the wave
-//   wf_trace      closest hit of every active path          (queue q_in)
-//   wf_shade<K>   emitters, light sample -> shadow ray, material sample ->
-//                 next ray, throughput update                 (q_in -> q_out,
-//                 shadow queue)
-//   wf_shadow<K>  any-hit test of the shadow rays; adds their radiance
-//   wf_splat<K>   adds every path's radiance to its pixel's XYZ film
-//   wf_finalize   film -> linear RGB in the reference's layout
+//   wf_finish<K>          ended paths of the last iteration -> XYZ of their
+//                         (sample, pixel) film entry
+//   wf_plan               how many new paths fit behind the queue
+//   wf_generate_stream<K> camera ray + hero wavelengths of the new paths,
+//                         appended to the queue
+//   wf_trace_*            closest hit of every queued path
+//   wf_shade<K>           emitters, light sample -> shadow ray, material
+//                         sample -> next ray; a continuing path is written
+//                         to the next position of the `out` queue, an
+//                         ended one to the ended list
+//   wf_shadow / wf_trace_persistent<true>
+//                         any-hit test of the shadow rays; an unoccluded
+//                         ray adds its radiance to its path (in `out` or in
+//                         the ended list)
 //
-// Each path draws its random numbers from its own counter-based stream in
-// the same order as Renderer::tracePath (src/renderer.cpp:64-146), so a
-// path's result does not depend on which kernel or slot processes it.
-// Paths are appended to the output queues with one atomic per warp
-// (ballot + popc).  The per-path state is SoA so a warp's accesses to one
-// field are coalesced.  Spectral state (throughput and radiance per hero
-// wavelength) lives in memory and is streamed one wavelength at a time, so
-// the shading kernel keeps no spectral arrays in registers.
+// then the host swaps `in` and `out`.  No path keeps a fixed slot, so no
+// access is scattered.  Each path draws its random numbers from its own
+// counter-based stream in the order of Renderer::tracePath
+// (src/renderer.cpp:64-146), and each (sample, pixel) result has its own
+// film entry summed in sample order, so the image does not depend on how
+// paths are scheduled.  Queue appends take one atomic per warp (ballot +
+// popc).
 #pragma once
 
 #include "lgpu_counters.cuh"
@@ -39,148 +45,90 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool pred) {
   return base + __popc(b & ((1u << lane) - 1u));
 }
 
+__device__ __forceinline__ Ray load_ray(const float* ray, uint32_t cap, uint32_t i) {
+  return make_ray(f3{ray[i], ray[cap + i], ray[2 * cap + i]},
+                  f3{ray[3 * cap + i], ray[4 * cap + i], ray[5 * cap + i]});
+}
+
+__device__ __forceinline__ void store_hit(const WaveState& w, uint32_t p, const HitRec& h) {
+  uint32_t const cap = w.cap;
+  float* hp = w.hit;
+  hp[0 * cap + p] = h.z;
+  hp[1 * cap + p] = __uint_as_float(h.obj);
+  hp[2 * cap + p] = __uint_as_float(h.face);
+  hp[3 * cap + p] = h.b0;
+  hp[4 * cap + p] = h.b1;
+  hp[5 * cap + p] = h.b2;
+  hp[6 * cap + p] = h.pl.x;
+  hp[7 * cap + p] = h.pl.y;
+  hp[8 * cap + p] = h.pl.z;
+}
+
+__device__ __forceinline__ void clear_hit(HitRec& h, float z) {
+  h.z = z;
+  h.obj = UINT32_MAX;
+  h.face = UINT32_MAX;
+  h.b0 = h.b1 = h.b2 = 0.f;
+  h.pl = f3{0.f, 0.f, 0.f};
+}
+
 // The non-template kernels get internal linkage: every translation unit
 // that instantiates the renderer carries its own copy.
 namespace {
 
-// ---- generate -------------------------------------------------------------------
-
-__global__ void __launch_bounds__(256) wf_generate(DevScene S, RenderArgs a, WaveState w, uint32_t k_hero,
-                                                   uint32_t sample_base, DevCounters* cnt) {
-  uint32_t const n = w.npix * w.n_samples;
-  uint32_t paths = 0;
-  float const omega = S.lambda_sup - S.lambda_inf;
-  const lgpu_camera& C = S.cam;
-  uint32_t const W = uint32_t(C.width);
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
-    uint32_t const s_local = p / w.npix;
-    uint32_t const pix = p - s_local * w.npix;
-    uint32_t const i = pix / W, j = pix - i * W;
-    uint64_t rng = lgpu_path_state(a.seed, (uint64_t(a.stream_tag) << 32) | pix,
-                                   uint64_t(a.spp_offset) + sample_base + s_local);
-    float const u = float(j) + lgpu_flt(&rng);
-    float const v = float(i) + lgpu_flt(&rng);
-    f3 const Fx = f3{C.base_x[0], C.base_x[1], C.base_x[2]};
-    f3 const Fy = f3{C.base_y[0], C.base_y[1], C.base_y[2]};
-    f3 const Fz = f3{C.base_z[0], C.base_z[1], C.base_z[2]};
-    f3 const P = f3{C.pos[0], C.pos[1], C.pos[2]};
-    float const cu = -0.5f * C.w + C.delta * u;
-    float const cv = -0.5f * C.h + C.delta * v;
-    f3 const wij = f3{P.x + Fx.x * cu + Fy.x * cv - C.D * Fz.x, P.y + Fx.y * cu + Fy.y * cv - C.D * Fz.y,
-                      P.z + Fx.z * cu + Fy.z * cv - C.D * Fz.z};
-    float const la = lgpu_flt(&rng) - 0.5f;
-    float const lb = lgpu_flt(&rng) - 0.5f;
-    float const dd = 2.f * C.dof;
-    f3 const wkl = f3{P.x + dd * (Fx.x * la + Fy.x * lb), P.y + dd * (Fx.y * la + Fy.y * lb),
-                      P.z + dd * (Fx.z * la + Fy.z * lb)};
-    f3 const dir = fnorm(f3{wij.x - wkl.x, wij.y - wkl.y, wij.z - wkl.z});
-    float const hero = S.lambda_inf + omega * lgpu_flt(&rng);
-    uint32_t const cap = w.cap;
-    w.ray[0 * cap + p] = wkl.x;
-    w.ray[1 * cap + p] = wkl.y;
-    w.ray[2 * cap + p] = wkl.z;
-    w.ray[3 * cap + p] = dir.x;
-    w.ray[4 * cap + p] = dir.y;
-    w.ray[5 * cap + p] = dir.z;
-    w.rng[p] = rng;
-    w.hero[p] = hero;
-    w.depth[p] = 0;
-    for (uint32_t k = 0; k < k_hero; k++) {
-      w.beta[k * cap + p] = 1.f;
-      w.acc[k * cap + p] = 0.f;
-    }
-    w.q_in[p] = p;
-    paths++;
-  }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *w.n_in = n;
-  TravStats const ts{0u, 0u, 0u, 0u};
-  flush_counters(cnt, 0u, paths, ts, 0u);
-}
-
-// ---- trace ------------------------------------------------------------------------
-
-__global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
-  extern __shared__ StackEntry smem_stack[];
-  StackEntry lm[kLocalStack];
-  StackEntry lstack[kStackCap];
-  StackEntry ltstack[kTlasStackCap];
-  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
-  TravStats ts{0u, 0u, 0u, 0u};
-  uint32_t rays = 0;
-  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
-  uint32_t const n = *w.n_in;
-  uint32_t const cap = w.cap;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    uint32_t const p = w.q_in[i];
-    Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
-                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
-    HitRec h;
-    h.z = kFltMax;
-    h.obj = UINT32_MAX;
-    h.face = UINT32_MAX;
-    h.b0 = h.b1 = h.b2 = 0.f;
-    h.pl = f3{0.f, 0.f, 0.f};
-    scene_trace<false>(S, r, h, UINT32_MAX, ref_order, st, lstack, ltstack, ts);
-    rays++;
-    float* hp = w.hit;
-    hp[0 * cap + p] = h.z;
-    hp[1 * cap + p] = __uint_as_float(h.obj);
-    hp[2 * cap + p] = __uint_as_float(h.face);
-    hp[3 * cap + p] = h.b0;
-    hp[4 * cap + p] = h.b1;
-    hp[5 * cap + p] = h.b2;
-    hp[6 * cap + p] = h.pl.x;
-    hp[7 * cap + p] = h.pl.y;
-    hp[8 * cap + p] = h.pl.z;
-  }
-  flush_counters(cnt, rays, 0u, ts, 0u);
-}
-
 // ---- streaming scheduler ------------------------------------------------------------
 
-// All slots free, no work handed out, no path in flight.
+// Empty queue, no work handed out, nothing ended.
 __global__ void wf_stream_init(WaveState w) {
-  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < w.cap; p += gridDim.x * blockDim.x)
-    w.free_list[p] = p;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    w.ctl[0] = w.cap;
-    w.ctl[1] = 0;
-    w.ctl[2] = 0;
     *w.n_in = 0;
+    *w.n_out = 0;
+    w.ctl[kCtlEnded] = 0;
+    w.ctl[kCtlNext] = 0;
   }
 }
 
-// Decides how many new paths the next generate starts: as many as there
-// are free slots, up to the remaining work items.
+// Runs after wf_finish: plans the next generate (as many new paths as fit
+// behind the queue, up to the remaining work items) and clears the
+// per-iteration counters.
 __global__ void wf_plan(WaveState w, uint32_t total) {
-  uint32_t const n_free = w.ctl[0], next = w.ctl[1];
+  uint32_t const n_in = *w.n_in, next = w.ctl[kCtlNext];
+  uint32_t const room = w.cap - n_in;
   uint32_t const left = total - next;
-  uint32_t const n_new = n_free < left ? n_free : left;
-  w.ctl[3] = n_new;
-  w.ctl[4] = next;
-  w.ctl[5] = n_free;
-  w.ctl[6] = *w.n_in;
-  w.ctl[0] = n_free - n_new;
-  w.ctl[1] = next + n_new;
-  *w.n_in += n_new;
+  uint32_t const n_new = room < left ? room : left;
+  w.ctl[kCtlNew] = n_new;
+  w.ctl[kCtlFirst] = next;
+  w.ctl[kCtlPos] = n_in;
+  w.ctl[kCtlNext] = next + n_new;
+  *w.n_in = n_in + n_new;
+  *w.n_out = 0;
+  w.ctl[kCtlShadow] = 0;
+  w.ctl[kCtlFetch] = 0;
+  w.ctl[kCtlFetch + 1] = 0;
+  w.ctl[kCtlFallback] = 0;
+  w.ctl[kCtlEnded] = 0;
 }
 
-// Starts the planned paths: work item q is sample q / npix of pixel
-// q % npix (all pixels of one sample before the next sample).
+// Starts the planned paths at the end of the queue: work item q is sample
+// q / npix of pixel q % npix (all pixels of one sample before the next).
+// Camera ray and hero wavelength as sample::camera and sample::spectrum
+// (cg.hpp:1534-1542, 1517-1531), random numbers drawn in the order of
+// Renderer::render (src/renderer.cpp:33-41).
+template <int K>
 __global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs a, WaveState w,
-                                                          uint32_t k_hero, uint32_t sample_base,
-                                                          DevCounters* cnt) {
-  uint32_t const n_new = w.ctl[3], first = w.ctl[4], top = w.ctl[5], qpos = w.ctl[6];
+                                                          uint32_t sample_base, DevCounters* cnt) {
+  uint32_t const n_new = w.ctl[kCtlNew], first = w.ctl[kCtlFirst], pos = w.ctl[kCtlPos];
   uint32_t paths = 0;
   float const omega = S.lambda_sup - S.lambda_inf;
   const lgpu_camera& C = S.cam;
   uint32_t const W = uint32_t(C.width);
   uint32_t const cap = w.cap;
+  PathBuf const& in = w.in;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_new; k += gridDim.x * blockDim.x) {
     uint32_t const q = first + k;
     uint32_t const s_local = q / w.npix;
     uint32_t const pix = q - s_local * w.npix;
-    uint32_t const p = w.free_list[top - 1 - k];
+    uint32_t const p = pos + k;
     uint32_t const i = pix / W, j = pix - i * W;
     uint64_t rng = lgpu_path_state(a.seed, (uint64_t(a.stream_tag) << 32) | pix,
                                    uint64_t(a.spp_offset) + sample_base + s_local);
@@ -201,59 +149,52 @@ __global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs
                       P.z + dd * (Fx.z * la + Fy.z * lb)};
     f3 const dir = fnorm(f3{wij.x - wkl.x, wij.y - wkl.y, wij.z - wkl.z});
     float const hero = S.lambda_inf + omega * lgpu_flt(&rng);
-    w.ray[0 * cap + p] = wkl.x;
-    w.ray[1 * cap + p] = wkl.y;
-    w.ray[2 * cap + p] = wkl.z;
-    w.ray[3 * cap + p] = dir.x;
-    w.ray[4 * cap + p] = dir.y;
-    w.ray[5 * cap + p] = dir.z;
-    w.rng[p] = rng;
-    w.hero[p] = hero;
-    w.depth[p] = 0;
-    w.pix[p] = pix;
-    w.samp[p] = s_local;
-    for (uint32_t kk = 0; kk < k_hero; kk++) {
-      w.beta[kk * cap + p] = 1.f;
-      w.acc[kk * cap + p] = 0.f;
+    in.ray[0 * cap + p] = wkl.x;
+    in.ray[1 * cap + p] = wkl.y;
+    in.ray[2 * cap + p] = wkl.z;
+    in.ray[3 * cap + p] = dir.x;
+    in.ray[4 * cap + p] = dir.y;
+    in.ray[5 * cap + p] = dir.z;
+    in.rng[p] = rng;
+    in.hero[p] = hero;
+    in.depth[p] = 0;
+    in.item[p] = q;
+#pragma unroll
+    for (int kk = 0; kk < K; kk++) {
+      in.beta[kk * cap + p] = 1.f;
+      in.acc[kk * cap + p] = 0.f;
     }
-    w.q_in[qpos + k] = p;
     paths++;
   }
   TravStats const ts{0u, 0u, 0u, 0u};
   flush_counters(cnt, 0u, paths, ts, 0u);
 }
 
-// Ended paths: their radiance goes to the (sample, pixel) film entry, their
-// slot back to the free list.
+// Ended paths: radiance splatted to XYZ (addHeroλ(λ, Li/prob),
+// src/renderer.cpp:44) into the path's (sample, pixel) film entry.
 template <int K>
 __global__ void __launch_bounds__(256) wf_finish(DevScene S, WaveState w, DevCounters* cnt) {
-  uint32_t const n = w.ctl[2];
+  uint32_t const n = w.ctl[kCtlEnded];
   float const omega = S.lambda_sup - S.lambda_inf;
   float const step = omega / float(K);
   float const prob_l = 1.f / omega;
+  uint32_t const cap = w.cap;
   uint32_t nonfinite = 0;
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    uint32_t const i = base + threadIdx.x;
-    bool const live = i < n;
-    uint32_t p = 0;
-    if (live) {
-      p = w.fin_list[i];
-      float const hero = w.hero[p];
-      float sx = 0.f, sy = 0.f, sz = 0.f;
-      bool finite = true;
-      for (int k = 0; k < K; k++) {
-        float const val = w.acc[k * w.cap + p] / prob_l;
-        finite = finite && isfinite(val);
-        splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
-      }
-      nonfinite += finite ? 0u : 1u;
-      size_t const o = 3 * (size_t(w.samp[p]) * w.npix + w.pix[p]);
-      w.sbuf[o] = sx;
-      w.sbuf[o + 1] = sy;
-      w.sbuf[o + 2] = sz;
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    float const hero = w.e_hero[e];
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+      float const val = w.e_acc[k * cap + e] / prob_l;
+      finite = finite && isfinite(val);
+      splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
     }
-    uint32_t const slot = warp_append(&w.ctl[0], live);
-    if (live) w.free_list[slot] = p;
+    nonfinite += finite ? 0u : 1u;
+    size_t const o = 3 * size_t(w.e_item[e]);
+    w.sbuf[o] = sx;
+    w.sbuf[o + 1] = sy;
+    w.sbuf[o + 2] = sz;
   }
   TravStats const ts{0u, 0u, 0u, 0u};
   flush_counters(cnt, 0u, 0u, ts, nonfinite);
@@ -275,26 +216,49 @@ __global__ void __launch_bounds__(256) wf_reduce(WaveState w, uint32_t n_samples
   }
 }
 
-// Persistent instance-BVH traversal of the extension rays (ANY = false,
-// queue q_in, hit records out) or the shadow rays (ANY = true, shadow
-// queue, unoccluded contributions added to the path radiance).  A lane that
-// finishes its ray takes the next one; idle lanes are refilled together with
-// one atomic per warp once kRefill of them are waiting.
-constexpr int kRefill = 8;
+// ---- trace ------------------------------------------------------------------------
 
-__device__ __forceinline__ void store_hit(const WaveState& w, uint32_t p, const HitRec& h) {
-  uint32_t const cap = w.cap;
-  float* hp = w.hit;
-  hp[0 * cap + p] = h.z;
-  hp[1 * cap + p] = __uint_as_float(h.obj);
-  hp[2 * cap + p] = __uint_as_float(h.face);
-  hp[3 * cap + p] = h.b0;
-  hp[4 * cap + p] = h.b1;
-  hp[5 * cap + p] = h.b2;
-  hp[6 * cap + p] = h.pl.x;
-  hp[7 * cap + p] = h.pl.y;
-  hp[8 * cap + p] = h.pl.z;
+// Closest hit of every queued path with one thread per ray (the reference's
+// linear object loop, or the instance BVH).
+__global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
+  extern __shared__ StackEntry smem_stack[];
+  StackEntry lm[kLocalStack];
+  StackEntry lstack[kStackCap];
+  StackEntry ltstack[kTlasStackCap];
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  TravStats ts{0u, 0u, 0u, 0u};
+  uint32_t rays = 0;
+  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
+  uint32_t const n = *w.n_in;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Ray const r = load_ray(w.in.ray, w.cap, i);
+    HitRec h;
+    clear_hit(h, kFltMax);
+    scene_trace<false>(S, r, h, UINT32_MAX, ref_order, st, lstack, ltstack, ts);
+    rays++;
+    store_hit(w, i, h);
+  }
+  flush_counters(cnt, rays, 0u, ts, 0u);
 }
+
+// Adds an unoccluded shadow ray's radiance to its path: target bit 31 set
+// means the ended list, else the `out` queue.
+template <int K>
+__device__ __forceinline__ void add_shadow(const WaveState& w, uint32_t s) {
+  uint32_t const t = w.s_target[s];
+  float* acc = (t & kEndedBit) ? w.e_acc : w.out.acc;
+  uint32_t const idx = t & ~kEndedBit;
+  uint32_t const cap = w.cap;
+#pragma unroll
+  for (int k = 0; k < K; k++) acc[k * cap + idx] += w.s_contrib[k * cap + s];
+}
+
+// Persistent instance-BVH traversal of the extension rays (ANY = false,
+// the `in` queue, hit records out) or the shadow rays (ANY = true,
+// unoccluded contributions added to their paths).  A lane that finishes its
+// ray takes the next one; idle lanes are refilled together with one atomic
+// per warp once kRefill of them are waiting.
+constexpr int kRefill = 8;
 
 template <bool ANY, int K>
 __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveState w, DevCounters* cnt) {
@@ -303,8 +267,8 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
-  uint32_t const n = ANY ? *w.n_shadow : *w.n_in;
-  uint32_t* fetch = ANY ? w.fetch + 1 : w.fetch;
+  uint32_t const n = ANY ? w.ctl[kCtlShadow] : *w.n_in;
+  uint32_t* fetch = w.ctl + kCtlFetch + (ANY ? 1 : 0);
   uint32_t const cap = w.cap;
   unsigned const FULL = 0xFFFFFFFFu;
   int const lane = threadIdx.x & 31;
@@ -325,22 +289,14 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
         if (my < n) {
           idx = my;
           if (ANY) {
-            t.w = make_ray(f3{w.sray[my], w.sray[cap + my], w.sray[2 * cap + my]},
-                           f3{w.sray[3 * cap + my], w.sray[4 * cap + my], w.sray[5 * cap + my]});
-            t.h.z = w.sray[6 * cap + my];
+            t.w = load_ray(w.sray, cap, my);
+            clear_hit(t.h, w.sray[6 * cap + my]);
             t.skip = __float_as_uint(w.sray[7 * cap + my]);
           } else {
-            uint32_t const p = w.q_in[my];
-            idx = p;
-            t.w = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
-                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
-            t.h.z = kFltMax;
+            t.w = load_ray(w.in.ray, cap, my);
+            clear_hit(t.h, kFltMax);
             t.skip = UINT32_MAX;
           }
-          t.h.obj = UINT32_MAX;
-          t.h.face = UINT32_MAX;
-          t.h.b0 = t.h.b1 = t.h.b2 = 0.f;
-          t.h.pl = f3{0.f, 0.f, 0.f};
           t.any = ANY;
           t.ilimit = UINT32_MAX;
           phase = 1;
@@ -357,10 +313,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
     if (active && trace_step<ANY>(S, t, st, ts)) {
       active = false;
       if (ANY) {
-        if (!t.hit_any) {
-          uint32_t const p = w.s_path[idx];
-          for (int k = 0; k < K; k++) w.acc[k * cap + p] += w.s_contrib[k * cap + p];
-        }
+        if (!t.hit_any) add_shadow<K>(w, idx);
         continue;
       }
       uint32_t const p = idx;
@@ -368,11 +321,8 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
         // an object below W's index is hit before the ray leaves W's bounds:
         // the reference skips W, so its answer is the closest hit without W
         if (t.hit_any) {
-          t.w = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
-                         f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
-          t.h.z = kFltMax;
-          t.h.obj = UINT32_MAX;
-          t.h.face = UINT32_MAX;
+          t.w = load_ray(w.in.ray, cap, p);
+          clear_hit(t.h, kFltMax);
           t.any = false;
           t.skip = wobj;
           t.ilimit = UINT32_MAX;
@@ -390,7 +340,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
         // over the lower-index objects up to the exit decides it; otherwise
         // the ray is re-traced with the linear object loop.
         if (t.n_inside != 1) {
-          w.fb_queue[atomicAdd(w.n_fb, 1u)] = p;
+          w.fb_queue[atomicAdd(w.ctl + kCtlFallback, 1u)] = p;
           continue;
         }
         store_hit(w, p, t.h);
@@ -418,29 +368,14 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(DevScene S, WaveState w
   StackEntry lstack[kStackCap];
   StackEntry ltstack[kTlasStackCap];
   TravStats ts{0u, 0u, 0u, 0u};
-  uint32_t const n = *w.n_fb;
-  uint32_t const cap = w.cap;
+  uint32_t const n = w.ctl[kCtlFallback];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t const p = w.fb_queue[i];
-    Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
-                           f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+    Ray const r = load_ray(w.in.ray, w.cap, p);
     HitRec h;
-    h.z = kFltMax;
-    h.obj = UINT32_MAX;
-    h.face = UINT32_MAX;
-    h.b0 = h.b1 = h.b2 = 0.f;
-    h.pl = f3{0.f, 0.f, 0.f};
+    clear_hit(h, kFltMax);
     scene_hit<false>(S, r, h, UINT32_MAX, true, lstack, ltstack, ts);
-    float* hp = w.hit;
-    hp[0 * cap + p] = h.z;
-    hp[1 * cap + p] = __uint_as_float(h.obj);
-    hp[2 * cap + p] = __uint_as_float(h.face);
-    hp[3 * cap + p] = h.b0;
-    hp[4 * cap + p] = h.b1;
-    hp[5 * cap + p] = h.b2;
-    hp[6 * cap + p] = h.pl.x;
-    hp[7 * cap + p] = h.pl.y;
-    hp[8 * cap + p] = h.pl.z;
+    store_hit(w, p, h);
   }
   flush_counters(cnt, 0u, 0u, ts, 0u);
 }
@@ -449,61 +384,71 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(DevScene S, WaveState w
 
 // ---- shade ------------------------------------------------------------------------
 
+// One vertex of Renderer::tracePath (src/renderer.cpp:64-146) for every
+// queued path: emitter hit (73-84), light importance sample with the MIS
+// power heuristic (87-113, its visibility left to the shadow kernel),
+// material importance sample with Russian roulette (115-143).
 template <int K>
 __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
   float const omega = S.lambda_sup - S.lambda_inf;
   float const step = omega / float(K);
+  PathBuf const& in = w.in;
+  PathBuf const& out = w.out;
+  enum : int { kEnd = 0, kEmit = 1, kScatter = 2 };
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t const i = base + threadIdx.x;
     bool const live = i < n;
-    bool cont = false, shadow = false;
-    uint32_t p = 0;
+    int kind = kEnd;
+    bool cont = false, shadow = false, needs_test = false;
     f3 sp = f3{0.f, 0.f, 0.f}, sd = f3{0.f, 0.f, 1.f};
     float stmax = 0.f;
     uint32_t sskip = UINT32_MAX;
-    f3 nd = f3{0.f, 0.f, 1.f}, np = f3{0.f, 0.f, 0.f};
-    float lis_scale = 0.f, m_scale = 0.f;
+    f3 np = f3{0.f, 0.f, 0.f}, nd = f3{0.f, 0.f, 1.f};
+    float lis_scale = 0.f, m_scale = 0.f, g_emit = 1.f, hero = 0.f;
+    uint64_t rng = 0;
+    uint32_t mat = 0, light = 0;
+    bool front = true;
+    MatSample ms;
+    ms.ok = false;
+    BsdfScalars bl{};
     if (live) {
-      p = w.q_in[i];
+      hero = in.hero[i];
       HitRec h;
-      h.obj = __float_as_uint(w.hit[cap + p]);
+      h.obj = __float_as_uint(w.hit[cap + i]);
       if (h.obj != UINT32_MAX) {
-        h.z = w.hit[p];
-        h.face = __float_as_uint(w.hit[2 * cap + p]);
-        h.b0 = w.hit[3 * cap + p];
-        h.b1 = w.hit[4 * cap + p];
-        h.b2 = w.hit[5 * cap + p];
-        h.pl = f3{w.hit[6 * cap + p], w.hit[7 * cap + p], w.hit[8 * cap + p]};
-        Ray const r = make_ray(f3{w.ray[p], w.ray[cap + p], w.ray[2 * cap + p]},
-                               f3{w.ray[3 * cap + p], w.ray[4 * cap + p], w.ray[5 * cap + p]});
+        h.z = w.hit[i];
+        h.face = __float_as_uint(w.hit[2 * cap + i]);
+        h.b0 = w.hit[3 * cap + i];
+        h.b1 = w.hit[4 * cap + i];
+        h.b2 = w.hit[5 * cap + i];
+        h.pl = f3{w.hit[6 * cap + i], w.hit[7 * cap + i], w.hit[8 * cap + i]};
+        Ray const r = load_ray(in.ray, cap, i);
         HitInfo const H = finalize_hit(S, r, h);
         f3 const un = fnorm(r.u);
         f3 const o = f3{-un.x, -un.y, -un.z};
         f3 const nn = H.front ? H.F.z : neg3(H.F.z);
-        const DevMaterial& m = S.mats[H.mat];
-        float const hero = w.hero[p];
+        mat = H.mat;
+        front = H.front;
+        const DevMaterial& m = S.mats[mat];
         if (m.type == LGPU_MAT_EMITTER || m.type == LGPU_MAT_DIREMITTER) {
-          float g = 1.f;
+          kind = kEmit;
           if (m.type == LGPU_MAT_DIREMITTER) {
             float const c = fdot(o, H.F.z);
-            g = powf(c >= 0.f ? c : 0.f, m.specular);
+            g_emit = powf(c >= 0.f ? c : 0.f, m.specular);
           }
-          for (int k = 0; k < K; k++) {
-            float const x = lam_coord(S, hero_lambda(S, hero, step, k));
-            w.acc[k * cap + p] += w.beta[k * cap + p] * (spec_at(S, m.spectrum[0], x) * g);
-          }
-        } else if (w.depth[p] <= a.max_scatter) {
-          uint64_t rng = w.rng[p];
-          uint32_t const li = uint32_t(lgpu_u64(&rng) % uint64_t(S.n_lights));
+        } else if (in.depth[i] <= a.max_scatter) {
+          kind = kScatter;
+          rng = in.rng[i];
+          light = uint32_t(lgpu_u64(&rng) % uint64_t(S.n_lights));
           float const prob_l = 1.f / float(S.n_lights);
-          const lgpu_light& L = S.lights[li];
+          const lgpu_light& L = S.lights[light];
           // light sample without its visibility (the shadow kernel applies it)
           LightSample ls = sample_light_unoccluded(S, L, H, rng, stmax, sskip);
           float const x0 = lam_coord(S, hero);
-          BsdfScalars const bl = bsdf_scalars(S, m, x0, ls.dir, o, nn, H.front);
-          MatSample const ms = sample_material(S, m, x0, H, o, a.sample_p, rng);
+          bl = bsdf_scalars(S, m, x0, ls.dir, o, nn, H.front);
+          ms = sample_material(S, m, x0, H, o, a.sample_p, rng);
           float w_L = 1.f, w_mat = 0.f;
           if (ms.ok) {
             float const p_L_mati = prob_for_light(S, L, H.p, ms.dir) * prob_l;
@@ -514,20 +459,8 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
           }
           lis_scale = ls.scale / (ls.prob * prob_l) * w_L;
           m_scale = ms.ok ? w_mat / ms.prob : 0.f;
-          bool const needs_test = stmax >= 0.f;
+          needs_test = stmax >= 0.f;
           shadow = needs_test && lis_scale != 0.f;
-          for (int k = 0; k < K; k++) {
-            float const l = hero_lambda(S, hero, step, k);
-            float const x = lam_coord(S, l);
-            float const coef = bsdf_k(S, m, bl, x, l, H.front);
-            float const rad = spec_at(S, L.spectrum, x);
-            float const b = w.beta[k * cap + p];
-            float const contrib = b * (rad * coef * lis_scale);
-            if (!needs_test) w.acc[k * cap + p] += contrib;
-            else w.s_contrib[k * cap + p] = contrib;  // slot p; gathered via s_path
-            if (ms.ok) w.beta[k * cap + p] = b * (mat_mult_k(S, m, ms, x, l, H.front) * m_scale);
-          }
-          w.rng[p] = rng;
           sp = H.p;
           sd = ls.dir;
           cont = ms.ok;
@@ -538,34 +471,63 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
         }
       }
     }
-    // compacted appends: next-bounce queue, ended paths and shadow queue
-    if (w.fin_list) {
-      bool const ended = live && !cont;
-      uint32_t const fo = warp_append(&w.ctl[2], ended);
-      if (ended) w.fin_list[fo] = p;
+    // compacted appends: next queue, ended list, shadow queue
+    bool const ended = live && !cont;
+    uint32_t const o_pos = warp_append(w.n_out, cont);
+    uint32_t const e_pos = warp_append(w.ctl + kCtlEnded, ended);
+    uint32_t const s_pos = warp_append(w.ctl + kCtlShadow, shadow);
+    if (!live) continue;
+    float* const acc_dst = cont ? out.acc + o_pos : w.e_acc + e_pos;
+    const DevMaterial& m = S.mats[mat];
+    if (kind == kScatter) {
+      const lgpu_light& L = S.lights[light];
+      for (int k = 0; k < K; k++) {
+        float const l = hero_lambda(S, hero, step, k);
+        float const x = lam_coord(S, l);
+        float const coef = bsdf_k(S, m, bl, x, l, front);
+        float const rad = spec_at(S, L.spectrum, x);
+        float const b = in.beta[k * cap + i];
+        float const contrib = b * (rad * coef * lis_scale);
+        float acc = in.acc[k * cap + i];
+        if (!needs_test) acc += contrib;
+        else if (shadow) w.s_contrib[k * cap + s_pos] = contrib;
+        if (cont) out.beta[k * cap + o_pos] = b * (mat_mult_k(S, m, ms, x, l, front) * m_scale);
+        acc_dst[k * cap] = acc;
+      }
+    } else if (kind == kEmit) {
+      for (int k = 0; k < K; k++) {
+        float const x = lam_coord(S, hero_lambda(S, hero, step, k));
+        acc_dst[k * cap] = in.acc[k * cap + i] + in.beta[k * cap + i] * (spec_at(S, m.spectrum[0], x) * g_emit);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; k++) acc_dst[k * cap] = in.acc[k * cap + i];
     }
-    uint32_t const qo = warp_append(w.n_out, cont);
     if (cont) {
-      w.q_out[qo] = p;
-      w.ray[0 * cap + p] = np.x;
-      w.ray[1 * cap + p] = np.y;
-      w.ray[2 * cap + p] = np.z;
-      w.ray[3 * cap + p] = nd.x;
-      w.ray[4 * cap + p] = nd.y;
-      w.ray[5 * cap + p] = nd.z;
-      w.depth[p] += 1;
+      out.ray[0 * cap + o_pos] = np.x;
+      out.ray[1 * cap + o_pos] = np.y;
+      out.ray[2 * cap + o_pos] = np.z;
+      out.ray[3 * cap + o_pos] = nd.x;
+      out.ray[4 * cap + o_pos] = nd.y;
+      out.ray[5 * cap + o_pos] = nd.z;
+      out.rng[o_pos] = rng;
+      out.hero[o_pos] = hero;
+      out.depth[o_pos] = in.depth[i] + 1;
+      out.item[o_pos] = in.item[i];
+    } else {
+      w.e_hero[e_pos] = hero;
+      w.e_item[e_pos] = in.item[i];
     }
-    uint32_t const so = warp_append(w.n_shadow, shadow);
     if (shadow) {
-      w.s_path[so] = p;
-      w.sray[0 * cap + so] = sp.x;
-      w.sray[1 * cap + so] = sp.y;
-      w.sray[2 * cap + so] = sp.z;
-      w.sray[3 * cap + so] = sd.x;
-      w.sray[4 * cap + so] = sd.y;
-      w.sray[5 * cap + so] = sd.z;
-      w.sray[6 * cap + so] = stmax;
-      w.sray[7 * cap + so] = __uint_as_float(sskip);
+      w.s_target[s_pos] = cont ? o_pos : (e_pos | kEndedBit);
+      w.sray[0 * cap + s_pos] = sp.x;
+      w.sray[1 * cap + s_pos] = sp.y;
+      w.sray[2 * cap + s_pos] = sp.z;
+      w.sray[3 * cap + s_pos] = sd.x;
+      w.sray[4 * cap + s_pos] = sd.y;
+      w.sray[5 * cap + s_pos] = sd.z;
+      w.sray[6 * cap + s_pos] = stmax;
+      w.sray[7 * cap + s_pos] = __uint_as_float(sskip);
     }
   }
   (void)cnt;
@@ -573,6 +535,7 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
 
 // ---- shadow -----------------------------------------------------------------------
 
+// Any-hit test of every shadow ray with one thread per ray.
 template <int K>
 __global__ void __launch_bounds__(128) wf_shadow(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
@@ -583,56 +546,18 @@ __global__ void __launch_bounds__(128) wf_shadow(DevScene S, WaveState w, uint32
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
   bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
-  uint32_t const n = *w.n_shadow;
+  uint32_t const n = w.ctl[kCtlShadow];
   uint32_t const cap = w.cap;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    Ray const r = make_ray(f3{w.sray[i], w.sray[cap + i], w.sray[2 * cap + i]},
-                           f3{w.sray[3 * cap + i], w.sray[4 * cap + i], w.sray[5 * cap + i]});
+    Ray const r = load_ray(w.sray, cap, i);
     HitRec h;
-    h.z = w.sray[6 * cap + i];
-    h.obj = UINT32_MAX;
+    clear_hit(h, w.sray[6 * cap + i]);
     uint32_t const skip = __float_as_uint(w.sray[7 * cap + i]);
     bool const occ = scene_trace<true>(S, r, h, skip, ref_order, st, lstack, ltstack, ts);
     rays++;
-    if (!occ) {
-      uint32_t const p = w.s_path[i];
-      for (int k = 0; k < K; k++) w.acc[k * cap + p] += w.s_contrib[k * cap + p];
-    }
+    if (!occ) add_shadow<K>(w, i);
   }
   flush_counters(cnt, rays, 0u, ts, 0u);
-}
-
-// ---- film ---------------------------------------------------------------------------
-
-template <int K>
-__global__ void __launch_bounds__(256) wf_splat(DevScene S, WaveState w, DevCounters* cnt) {
-  uint32_t nonfinite = 0;
-  float const omega = S.lambda_sup - S.lambda_inf;
-  float const step = omega / float(K);
-  float const prob_l = 1.f / omega;
-  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < w.npix; pix += gridDim.x * blockDim.x) {
-    float X = w.film[3 * pix], Y = w.film[3 * pix + 1], Z = w.film[3 * pix + 2];
-    for (uint32_t s = 0; s < w.n_samples; s++) {
-      uint32_t const p = s * w.npix + pix;
-      float const hero = w.hero[p];
-      float sx = 0.f, sy = 0.f, sz = 0.f;
-      bool finite = true;
-      for (int k = 0; k < K; k++) {
-        float const val = w.acc[k * w.cap + p] / prob_l;
-        finite = finite && isfinite(val);
-        splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
-      }
-      nonfinite += finite ? 0u : 1u;
-      X += sx;
-      Y += sy;
-      Z += sz;
-    }
-    w.film[3 * pix] = X;
-    w.film[3 * pix + 1] = Y;
-    w.film[3 * pix + 2] = Z;
-  }
-  TravStats const ts{0u, 0u, 0u, 0u};
-  flush_counters(cnt, 0u, 0u, ts, nonfinite);
 }
 
 }  // namespace lgpu
