@@ -190,6 +190,70 @@ def kernel_roofline(ctx, spp, B, p, stream):
             "kernels_ms": {KERNEL_NAMES[i].split(" (")[0]: ks[i]["ms"] for i in range(3)}}
 
 
+BATCH_DESC = ("64 jobs: box room (10 wall tris + 2 blocks, quad light) with U[1,128] instances of a "
+              "displaced icosphere of subdivision 5-7 (20K-328K tris each), resolution from "
+              "128^2/256^2/512^2/1024^2, spp log-uniform 4-256, bounces U[4,32], p=0.8, "
+              "4 hero wavelengths on 380-780 nm (81 bins)")
+
+
+def run_batched(ctx_cls, device, n_jobs=64):
+    """Config 3: the 64 jobs in one batched launch vs the same jobs as
+    back-to-back plain launches (lgpu_render_batch_device with one job),
+    scenes resident, device time by CUDA events; both produce identical
+    images (checked), so per-job RMSE is equal."""
+    import numpy as np
+    import torch
+
+    from lambda_b200 import synth
+    from lambda_b200.scene import SpectralConfig, flatten, load_nls
+    root = os.path.join(tempfile.gettempdir(), "lgpu_bench", "batch")
+    cfg = SpectralConfig(n_bins=81, lambda_inf=380.0, lambda_sup=780.0, hero_k=4)
+    specs = synth.batch_jobs(n_jobs)
+    flats = []
+    for k, j in enumerate(specs):
+        nls = synth.batch_job(os.path.join(root, "job%02d" % k), j["n_instances"], j["subdiv"],
+                              os.path.join(root, "meshes"), seed=j["seed"], width=j["width"])
+        flats.append(flatten(load_nls(nls, cfg)))
+    ctx = ctx_cls(device)
+    ctx.upload_many(flats)
+    jobs = [dict(scene=k, spp=j["spp"], max_scatterings=j["max_scatterings"], sample_p=j["sample_p"],
+                 seed=j["seed"]) for k, j in enumerate(specs)]
+    outs = [torch.empty(j["width"] * j["width"] * 3, dtype=torch.float32, device="cuda") for j in specs]
+    seq = [torch.empty_like(o) for o in outs]
+    ptrs = [o.data_ptr() for o in outs]
+    paths = sum(j["width"] * j["width"] * j["spp"] for j in specs)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+
+    def timed(fn):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    def batched():
+        ctx.render_batch_device(jobs, ptrs, stream=stream.cuda_stream)
+
+    def sequential():
+        for j, o in zip(jobs, seq):
+            ctx.render_batch_device([j], [o.data_ptr()], stream=stream.cuda_stream)
+
+    batched()
+    launches = ctx.stats()["launches"]
+    sequential()
+    t_b = timed(batched)
+    t_s = timed(sequential)
+    equal = all(torch.equal(a, b) for a, b in zip(outs, seq))
+    return {"value": paths / t_b / 1e6, "unit": UNIT, "sequential_value": paths / t_s / 1e6,
+            "speedup": t_s / t_b, "batched_s": t_b, "sequential_s": t_s, "paths": paths,
+            "jobs": n_jobs, "images_identical": bool(equal), "gpu_launches": int(launches),
+            "workload": BATCH_DESC}
+
+
 def cpu_reference_sample(nls, w, budget_s, fast=True):
     """Times the reference's own pixel loop (oracle/_ref, -O3 OpenMP build)
     over rows spread across the image; returns (paths/s, cores, sample)."""
@@ -346,6 +410,8 @@ def run_device(args, w):
             "e2e": e2e, "roofline": roofline, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["batched"] = run_batched(Context, local)
     if rank == 0 and world == 1 and not args.no_baseline:
         from oracle import refharness
         if refharness.available(fast=True):
@@ -370,6 +436,7 @@ def main():
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--width", type=int, default=None, help="frame width (profiling)")
     ap.add_argument("--no-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential run")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="seconds of reference CPU work per sampled step")
     args = ap.parse_args()

@@ -263,6 +263,34 @@ int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linr
 int lgpu_render_device(lgpu_ctx* ctx, const lgpu_render_params* params,
                        float* d_out_linrgb, void* stream);
 
+/* Scene table for batched renders: uploads n scenes, scene k into slot k,
+   replacing whatever was uploaded before (lgpu_upload_scene(ctx, s) is
+   lgpu_upload_scenes(ctx, &s, 1); lgpu_render and lgpu_trace_closest use
+   slot 0).  All scenes must have the same spectral hero_k. */
+int lgpu_upload_scenes(lgpu_ctx* ctx, const lgpu_scene* const* scenes, uint32_t n);
+
+/* One job of a batched render: a slot of the scene table, the settings of
+   Renderer::render for it, and its output (that scene's
+   cam.width*cam.height*3 floats of linear RGB, row 0 at the top). */
+typedef struct lgpu_job {
+  uint32_t scene;
+  uint32_t reserved;
+  lgpu_render_params params;
+  float* out;
+} lgpu_job;
+
+/* Renders n jobs in one streaming wavefront: paths of all jobs share the
+   queues, so small jobs and the tails of large ones keep the GPU busy
+   (the batched form of Renderer::render, src/renderer.cpp:14-61; the
+   reference renders one scene per call).  Every job's image is identical to
+   lgpu_render of its scene with the same params.  A single job takes the
+   plain path.  lgpu_render_batch: outputs in host memory;
+   lgpu_render_batch_device: outputs in device memory, on `stream` (NULL:
+   the context's stream).  The kernel counters of lgpu_get_stats cover the
+   whole batch.  LGPU_ERR_TOO_LARGE if the jobs hold 2^31 pixels or more. */
+int lgpu_render_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n);
+int lgpu_render_batch_device(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, void* stream);
+
 /* intersect::scene (cg.hpp:1469-1489) on n rays given as 6 floats each
    (origin xyz, direction xyz) in host memory; writes n lgpu_hit. */
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,

@@ -97,6 +97,11 @@ class RenderParams(ctypes.Structure):
                 ("reserved", ctypes.c_uint32)]
 
 
+class Job(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("params", RenderParams), ("out", ctypes.c_void_p)]
+
+
 class Hit(ctypes.Structure):
     _fields_ = [("t", ctypes.c_float), ("obj", ctypes.c_uint32), ("face", ctypes.c_uint32),
                 ("mat", ctypes.c_uint32), ("p", ctypes.c_float * 3), ("n", ctypes.c_float * 3),
@@ -126,6 +131,9 @@ SIGNATURES = {
     "lgpu_destroy": (None, [_vp]),
     "lgpu_last_error": (ctypes.c_char_p, [_vp]),
     "lgpu_upload_scene": (ctypes.c_int, [_vp, ctypes.POINTER(Scene)]),
+    "lgpu_upload_scenes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.POINTER(Scene)), ctypes.c_uint32]),
+    "lgpu_render_batch": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32]),
+    "lgpu_render_batch_device": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, _vp]),
     "lgpu_render": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp]),
     "lgpu_render_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp]),
     "lgpu_trace_closest": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),

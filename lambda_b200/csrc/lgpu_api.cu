@@ -25,17 +25,9 @@ struct DevArray {
   }
 };
 
-}  // namespace
-
-struct lgpu_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  std::string err;
-  bool has_scene = false;
+// The device arrays of one uploaded scene.
+struct SceneSlot {
   DevScene S{};
-  lgpu_stats stats{};
-  // scene arrays
   DevArray<DevObject> objects;
   DevArray<DevMesh> meshes;
   DevArray<WideNode> nodes;
@@ -46,6 +38,40 @@ struct lgpu_ctx {
   DevArray<lgpu_light> lights;
   DevArray<uint32_t> tlas_objects;
   DevArray<float> cmf;
+  uint64_t bytes = 0;
+  void release() {
+    objects.release();
+    meshes.release();
+    nodes.release();
+    tris.release();
+    shade.release();
+    spectra.release();
+    mats.release();
+    lights.release();
+    tlas_objects.release();
+    cmf.release();
+    S = DevScene{};
+    bytes = 0;
+  }
+};
+
+}  // namespace
+
+struct lgpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::string err;
+  bool has_scene = false;
+  DevScene S{};
+  lgpu_stats stats{};
+  // the scene table (lgpu_upload_scenes); S is a copy of slot 0's DevScene
+  std::vector<SceneSlot> slots;
+  // batch tables (lgpu_render_batch)
+  DevArray<DevJob> jobs;
+  DevArray<uint64_t> job_items;
+  DevArray<uint32_t> job_pixels;
+  DevArray<float> batch_out;
   // working buffers
   DevArray<float> out;
   // wavefront state (lgpu_wave.cuh), sized for the largest frame rendered
@@ -62,16 +88,9 @@ struct lgpu_ctx {
   bool timer_ready = false;
 
   void release_scene() {
-    objects.release();
-    meshes.release();
-    nodes.release();
-    tris.release();
-    shade.release();
-    spectra.release();
-    mats.release();
-    lights.release();
-    tlas_objects.release();
-    cmf.release();
+    for (SceneSlot& sl : slots) sl.release();
+    slots.clear();
+    S = DevScene{};
     has_scene = false;
   }
 };
@@ -171,9 +190,10 @@ struct Carver {
 };
 
 // Lays out the wavefront buffers for queue capacity cap, K hero
-// wavelengths, npix pixels and ns samples per chunk; with base == nullptr
-// it only counts the bytes.
-size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint32_t ns, WaveState& ws) {
+// wavelengths, npix pixels and a chunk of sbuf_items work items; with
+// base == nullptr it only counts the bytes.
+size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint64_t sbuf_items, bool batch,
+                   WaveState& ws) {
   Carver c{base};
   size_t const n = cap;
   for (PathBuf* pb : {&ws.in, &ws.out}) {
@@ -182,6 +202,7 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint3
     pb->hero = c.take<float>(n);
     pb->depth = c.take<uint32_t>(n);
     pb->item = c.take<uint32_t>(n);
+    pb->job = batch ? c.take<uint32_t>(n) : nullptr;
     pb->beta = c.take<float>(size_t(K) * n);
     pb->acc = c.take<float>(size_t(K) * n);
   }
@@ -189,58 +210,45 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint3
   ws.e_acc = c.take<float>(size_t(K) * n);
   ws.e_hero = c.take<float>(n);
   ws.e_item = c.take<uint32_t>(n);
+  ws.e_job = batch ? c.take<uint32_t>(n) : nullptr;
   ws.sray = c.take<float>(8 * n);
   ws.s_target = c.take<uint32_t>(n);
   ws.s_contrib = c.take<float>(size_t(K) * n);
+  ws.s_job = batch ? c.take<uint32_t>(n) : nullptr;
   ws.fb_queue = c.take<uint32_t>(n);
   ws.ctl = c.take<uint32_t>(kCtlWords);
   ws.film = c.take<float>(3 * size_t(npix));
-  ws.sbuf = c.take<float>(3 * size_t(npix) * ns);
+  ws.sbuf = c.take<float>(3 * size_t(sbuf_items));
   return c.off;
 }
 
-// Sizes the wavefront buffers for a frame of npix pixels and fills ws.
-int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint32_t spp, WaveState& ws) {
+// paths in flight: about 2^21, fewer for small renders
+constexpr uint64_t kQueueCap = uint64_t(1) << 21;
+// the (sample, pixel) film buffer of one chunk stays under 2 GiB
+constexpr uint64_t kSbufBytes = uint64_t(1) << 31;
+
+// Sizes the wavefront buffers for npix pixels, n_items work items in chunks
+// of chunk_items, and fills ws.
+int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint64_t n_items, uint64_t chunk_items, bool batch,
+                WaveState& ws) {
   uint32_t const K = ctx->S.hero_k;
-  // paths in flight: about 2^21, fewer for small frames
-  uint64_t const work = uint64_t(npix) * spp;
-  uint32_t const cap = uint32_t(work < (1u << 21) ? work : (1u << 21));
-  // samples per chunk: the (sample, pixel) film buffer stays under 2 GiB
-  uint64_t const max_ns = (uint64_t(1) << 31) / (12ull * npix);
-  uint32_t const ns = uint32_t(spp < max_ns ? spp : (max_ns ? max_ns : 1));
-  size_t const bytes = wave_layout(nullptr, cap, K, npix, ns, ws);
+  uint32_t const cap = uint32_t(n_items < kQueueCap ? n_items : kQueueCap);
+  size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, ws);
   cudaError_t const e = ensure(ctx->w_arena, bytes);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront buffers");
-  wave_layout(ctx->w_arena.ptr, cap, K, npix, ns, ws);
+  wave_layout(ctx->w_arena.ptr, cap, K, npix, chunk_items, batch, ws);
   ws.cap = cap;
   ws.npix = npix;
-  ws.n_samples = ns;
+  ws.n_samples = 0;
+  ws.c0 = 0;
   ws.n_in = ws.ctl + kCtlCountA;
   ws.n_out = ws.ctl + kCtlCountB;
   ws.h_ctl = ctx->h_ctl;
   return LGPU_OK;
 }
 
-int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaStream_t st) {
-  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
-  if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
-  RenderArgs a{};
-  a.spp = p->spp;
-  a.max_scatter = p->max_scatterings;
-  a.sample_p = p->sample_p;
-  a.flags = p->flags;
-  a.seed = p->seed;
-  a.spp_offset = p->spp_offset;
-  a.pixel_begin = 0;
-  a.pixel_count = uint32_t(ctx->S.cam.width * ctx->S.cam.height);
-  WaveState ws{};
-  WaveState* wave = nullptr;
-  if (!(p->flags & LGPU_FLAG_MEGAKERNEL)) {
-    int const r = ensure_wave(ctx, a.pixel_count, a.spp, ws);
-    if (r != LGPU_OK) return r;
-    wave = &ws;
-  }
-  bool const timing = (p->flags & LGPU_FLAG_KERNEL_TIMING) && wave;
+// Creates the timing events on first use and resets the launch record.
+int prepare_timer(lgpu_ctx* ctx, bool timing) {
   if (timing && !ctx->timer_ready) {
     for (auto& k : ctx->timer.ev)
       for (auto& s : k)
@@ -249,18 +257,182 @@ int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaSt
     ctx->timer_ready = true;
   }
   ctx->timer.reset(timing);
-  KernelTimer* const timer = &ctx->timer;
+  return LGPU_OK;
+}
+
+RenderArgs render_args(const lgpu_render_params* p, const DevScene& S) {
+  RenderArgs a{};
+  a.spp = p->spp;
+  a.max_scatter = p->max_scatterings;
+  a.sample_p = p->sample_p;
+  a.flags = p->flags;
+  a.seed = p->seed;
+  a.spp_offset = p->spp_offset;
+  a.pixel_begin = 0;
+  a.pixel_count = uint32_t(S.cam.width * S.cam.height);
+  a.stream_tag = 0;
+  return a;
+}
+
+// Renders scene S into d_out (device, linear RGB) on stream st.
+int render_scene(lgpu_ctx* ctx, const DevScene& S, const lgpu_render_params* p, float* d_out,
+                 cudaStream_t st) {
+  if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  RenderArgs const a = render_args(p, S);
+  WaveState ws{};
+  WaveState* wave = nullptr;
+  if (!(p->flags & LGPU_FLAG_MEGAKERNEL)) {
+    uint64_t const npix = a.pixel_count;
+    uint64_t const max_ns = kSbufBytes / (12 * npix);
+    uint32_t const ns = uint32_t(a.spp < max_ns ? a.spp : (max_ns ? max_ns : 1));
+    int const r = ensure_wave(ctx, a.pixel_count, npix * a.spp, npix * ns, false, ws);
+    if (r != LGPU_OK) return r;
+    ws.n_samples = ns;
+    wave = &ws;
+  }
+  if (int r = prepare_timer(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) && wave)) return r;
   cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  if (e == cudaSuccess) e = launch_render(ctx->S, a, wave, d_out, ctx->counters, st, timer);
+  if (e == cudaSuccess) e = launch_render(S, a, wave, d_out, ctx->counters, st, &ctx->timer);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return LGPU_OK;
 }
 
+int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaStream_t st) {
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  return render_scene(ctx, ctx->S, p, d_out, st);
+}
+
+// Renders the jobs (outputs d_outs, device) in one streaming wavefront; a
+// single job takes the plain path.
+int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_outs, cudaStream_t st) {
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  bool timing = false, linear = false;
+  for (uint32_t k = 0; k < n; k++) {
+    if (jobs[k].scene >= ctx->slots.size())
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": no such scene");
+    if (jobs[k].params.spp == 0)
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": spp must be >= 1");
+    if (!d_outs[k]) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": null output");
+    timing = timing || (jobs[k].params.flags & LGPU_FLAG_KERNEL_TIMING);
+    linear = linear || (jobs[k].params.flags & LGPU_FLAG_REFERENCE_ORDER);
+  }
+  if (n == 1) return render_scene(ctx, ctx->slots[jobs[0].scene].S, &jobs[0].params, d_outs[0], st);
+  std::vector<DevJob> hj(n);
+  std::vector<uint64_t> items(n + 1);
+  std::vector<uint32_t> pixels(n + 1);
+  uint64_t g = 0, px = 0;
+  for (uint32_t k = 0; k < n; k++) {
+    DevJob& d = hj[k];
+    d.S = ctx->slots[jobs[k].scene].S;
+    d.a = render_args(&jobs[k].params, d.S);
+    d.npix = d.a.pixel_count;
+    d.item_base = g;
+    d.pix_base = uint32_t(px);
+    d.out = d_outs[k];
+    items[k] = g;
+    pixels[k] = uint32_t(px);
+    g += uint64_t(d.npix) * d.a.spp;
+    px += d.npix;
+    if (px >= (uint64_t(1) << 31))
+      return fail(ctx, LGPU_ERR_TOO_LARGE, "a batch holds at most 2^31 pixels in all");
+  }
+  items[n] = g;
+  pixels[n] = uint32_t(px);
+  uint64_t const max_chunk = kSbufBytes / 12;
+  uint64_t const chunk = g < max_chunk ? g : max_chunk;
+  cudaError_t e = ensure(ctx->jobs, n);
+  if (e == cudaSuccess) e = ensure(ctx->job_items, n + 1);
+  if (e == cudaSuccess) e = ensure(ctx->job_pixels, n + 1);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch tables");
+  e = cudaMemcpyAsync(ctx->jobs.ptr, hj.data(), n * sizeof(DevJob), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->job_items.ptr, items.data(), (n + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->job_pixels.ptr, pixels.data(), (n + 1) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                        st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch tables");
+  WaveState ws{};
+  if (int r = ensure_wave(ctx, uint32_t(px), g, chunk, true, ws)) return r;
+  if (int r = prepare_timer(ctx, timing)) return r;
+  e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
+  if (e == cudaSuccess)
+    e = launch_batch(ctx->S.hero_k, ctx->jobs.ptr, ctx->job_items.ptr, ctx->job_pixels.ptr, n, g, chunk, linear,
+                     &ws, ctx->counters, st, &ctx->timer);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
+  // the host tables must outlive their asynchronous copies
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch launch");
+  return LGPU_OK;
+}
+
+bool batch_timing(const lgpu_job* jobs, uint32_t n) {
+  for (uint32_t k = 0; k < n; k++)
+    if ((jobs[k].params.flags & LGPU_FLAG_KERNEL_TIMING) && !(n == 1 && (jobs[k].params.flags & LGPU_FLAG_MEGAKERNEL)))
+      return true;
+  return false;
+}
+
 // per-kernel timing applies to the wavefront kernels only
 bool timing_requested(const lgpu_render_params* p) {
   return (p->flags & LGPU_FLAG_KERNEL_TIMING) && !(p->flags & LGPU_FLAG_MEGAKERNEL);
+}
+
+// Lays out one scene on the host and copies it into a scene slot.
+int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
+  HostLayout L;
+  std::string err;
+  int const rc = make_layout(scene, L, err);
+  if (rc != LGPU_OK) return fail(ctx, rc, err);
+  cudaStream_t const st = ctx->stream;
+  cudaError_t e = upload(sl.objects, L.objects, st);
+  if (e == cudaSuccess) e = upload(sl.meshes, L.meshes, st);
+  if (e == cudaSuccess) e = upload(sl.nodes, L.nodes, st);
+  if (e == cudaSuccess) e = upload(sl.tris, L.tris, st);
+  if (e == cudaSuccess) e = upload(sl.shade, L.shade, st);
+  if (e == cudaSuccess) e = upload(sl.spectra, L.spectra, st);
+  if (e == cudaSuccess) e = upload(sl.mats, L.mats, st);
+  if (e == cudaSuccess) e = upload(sl.lights, L.lights, st);
+  if (e == cudaSuccess) e = upload(sl.tlas_objects, L.tlas_objects, st);
+  if (e == cudaSuccess) e = upload(sl.cmf, L.cmf, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "scene upload");
+  DevScene& S = sl.S;
+  S = DevScene{};
+  S.objects = sl.objects.ptr;
+  S.meshes = sl.meshes.ptr;
+  S.nodes = sl.nodes.ptr;
+  S.tris = sl.tris.ptr;
+  S.shade = sl.shade.ptr;
+  S.spectra = sl.spectra.ptr;
+  S.mats = sl.mats.ptr;
+  S.lights = sl.lights.ptr;
+  S.tlas_objects = sl.tlas_objects.ptr;
+  S.n_objects = scene.n_objects;
+  S.n_meshes = scene.n_meshes;
+  S.n_materials = scene.n_materials;
+  S.n_lights = scene.n_lights;
+  S.tlas_root = L.tlas_root;
+  S.max_stack = L.max_stack;
+  S.tlas_max_stack = L.tlas_max_stack;
+  S.n_bins = scene.spec.n_bins;
+  S.hero_k = scene.spec.hero_k;
+  S.lambda_inf = scene.spec.lambda_inf;
+  S.lambda_sup = scene.spec.lambda_sup;
+  // coefficientλ::Δ = (sup-inf)/(n-1) (cg.hpp:246)
+  S.lambda_delta = (S.lambda_sup - S.lambda_inf) / float(S.n_bins - 1);
+  S.cmf = sl.cmf.ptr;
+  S.cam = scene.cam;
+  std::memcpy(S.tlas_bounds, L.tlas_bounds, sizeof(S.tlas_bounds));
+  if (L.max_stack > ctx->stats.max_stack) ctx->stats.max_stack = L.max_stack;
+  sl.bytes = L.objects.size() * sizeof(DevObject) + L.meshes.size() * sizeof(DevMesh) +
+             L.nodes.size() * sizeof(WideNode) + L.tris.size() * sizeof(TriSlot) +
+             L.shade.size() * sizeof(FaceShade) + L.spectra.size() * sizeof(float) +
+             L.mats.size() * sizeof(DevMaterial) + L.lights.size() * sizeof(lgpu_light) +
+             L.tlas_objects.size() * sizeof(uint32_t) + L.cmf.size() * sizeof(float);
+  return LGPU_OK;
 }
 
 }  // namespace
@@ -323,63 +495,32 @@ const char* lgpu_last_error(const lgpu_ctx* ctx) { return ctx ? ctx->err.c_str()
 
 int lgpu_upload_scene(lgpu_ctx* ctx, const lgpu_scene* scene) {
   if (!ctx || !scene) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  return lgpu_upload_scenes(ctx, &scene, 1);
+}
+
+int lgpu_upload_scenes(lgpu_ctx* ctx, const lgpu_scene* const* scenes, uint32_t n) {
+  if (!ctx || !scenes || n == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument or no scene");
   if (int r = bind_device(ctx)) return r;
-  HostLayout L;
-  std::string err;
-  int const rc = make_layout(*scene, L, err);
-  if (rc != LGPU_OK) return fail(ctx, rc, err);
+  for (uint32_t k = 0; k < n; k++) {
+    if (!scenes[k]) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null scene " + std::to_string(k));
+    if (scenes[k]->spec.hero_k != scenes[0]->spec.hero_k)
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "all scenes of a table need the same hero-wavelength count");
+  }
   cudaStreamSynchronize(ctx->stream);
   ctx->release_scene();
-  cudaStream_t const st = ctx->stream;
-  cudaError_t e = upload(ctx->objects, L.objects, st);
-  if (e == cudaSuccess) e = upload(ctx->meshes, L.meshes, st);
-  if (e == cudaSuccess) e = upload(ctx->nodes, L.nodes, st);
-  if (e == cudaSuccess) e = upload(ctx->tris, L.tris, st);
-  if (e == cudaSuccess) e = upload(ctx->shade, L.shade, st);
-  if (e == cudaSuccess) e = upload(ctx->spectra, L.spectra, st);
-  if (e == cudaSuccess) e = upload(ctx->mats, L.mats, st);
-  if (e == cudaSuccess) e = upload(ctx->lights, L.lights, st);
-  if (e == cudaSuccess) e = upload(ctx->tlas_objects, L.tlas_objects, st);
-  if (e == cudaSuccess) e = upload(ctx->cmf, L.cmf, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) {
-    ctx->release_scene();
-    return cuda_fail(ctx, e, "scene upload");
+  ctx->slots.resize(n);
+  ctx->stats.max_stack = 0;
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < n; k++) {
+    int const rc = upload_slot(ctx, ctx->slots[k], *scenes[k]);
+    if (rc != LGPU_OK) {
+      ctx->release_scene();
+      return rc;
+    }
+    total += ctx->slots[k].bytes;
   }
-  DevScene& S = ctx->S;
-  S = DevScene{};
-  S.objects = ctx->objects.ptr;
-  S.meshes = ctx->meshes.ptr;
-  S.nodes = ctx->nodes.ptr;
-  S.tris = ctx->tris.ptr;
-  S.shade = ctx->shade.ptr;
-  S.spectra = ctx->spectra.ptr;
-  S.mats = ctx->mats.ptr;
-  S.lights = ctx->lights.ptr;
-  S.tlas_objects = ctx->tlas_objects.ptr;
-  S.n_objects = scene->n_objects;
-  S.n_meshes = scene->n_meshes;
-  S.n_materials = scene->n_materials;
-  S.n_lights = scene->n_lights;
-  S.tlas_root = L.tlas_root;
-  S.max_stack = L.max_stack;
-  S.tlas_max_stack = L.tlas_max_stack;
-  S.n_bins = scene->spec.n_bins;
-  S.hero_k = scene->spec.hero_k;
-  S.lambda_inf = scene->spec.lambda_inf;
-  S.lambda_sup = scene->spec.lambda_sup;
-  // coefficientλ::Δ = (sup-inf)/(n-1) (cg.hpp:246)
-  S.lambda_delta = (S.lambda_sup - S.lambda_inf) / float(S.n_bins - 1);
-  S.cmf = ctx->cmf.ptr;
-  S.cam = scene->cam;
-  std::memcpy(S.tlas_bounds, L.tlas_bounds, sizeof(S.tlas_bounds));
-  ctx->stats.max_stack = L.max_stack;
-  ctx->stats.upload_bytes =
-      L.objects.size() * sizeof(DevObject) + L.meshes.size() * sizeof(DevMesh) +
-      L.nodes.size() * sizeof(WideNode) + L.tris.size() * sizeof(TriSlot) +
-      L.shade.size() * sizeof(FaceShade) + L.spectra.size() * sizeof(float) +
-      L.mats.size() * sizeof(DevMaterial) + L.lights.size() * sizeof(lgpu_light) +
-      L.tlas_objects.size() * sizeof(uint32_t) + L.cmf.size() * sizeof(float);
+  ctx->S = ctx->slots[0].S;
+  ctx->stats.upload_bytes = total;
   ctx->has_scene = true;
   return LGPU_OK;
 }
@@ -409,6 +550,46 @@ int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linr
   e = cudaMemcpyAsync(out_linrgb, ctx->out.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render readback");
   return collect(ctx, "render", timing_requested(params));
+}
+
+int lgpu_render_batch_device(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, void* stream) {
+  if (!ctx || !jobs || n == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument or no job");
+  if (int r = bind_device(ctx)) return r;
+  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  std::vector<float*> outs(n);
+  for (uint32_t k = 0; k < n; k++) outs[k] = jobs[k].out;
+  int const rc = batch_impl(ctx, jobs, n, outs.data(), st);
+  if (rc != LGPU_OK) return rc;
+  if (st != ctx->stream) {
+    cudaError_t const e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "render batch");
+  }
+  return collect(ctx, "render batch", batch_timing(jobs, n));
+}
+
+int lgpu_render_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n) {
+  if (!ctx || !jobs || n == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument or no job");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  std::vector<size_t> off(n + 1, 0);
+  for (uint32_t k = 0; k < n; k++) {
+    if (jobs[k].scene >= ctx->slots.size())
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": no such scene");
+    if (!jobs[k].out) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": null output");
+    const lgpu_camera& c = ctx->slots[jobs[k].scene].S.cam;
+    off[k + 1] = off[k] + size_t(c.width) * c.height * 3;
+  }
+  cudaError_t e = ensure(ctx->batch_out, off[n]);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch output buffer");
+  std::vector<float*> outs(n);
+  for (uint32_t k = 0; k < n; k++) outs[k] = ctx->batch_out.ptr + off[k];
+  int const rc = batch_impl(ctx, jobs, n, outs.data(), ctx->stream);
+  if (rc != LGPU_OK) return rc;
+  for (uint32_t k = 0; k < n && e == cudaSuccess; k++)
+    e = cudaMemcpyAsync(jobs[k].out, outs[k], (off[k + 1] - off[k]) * sizeof(float), cudaMemcpyDeviceToHost,
+                        ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "batch readback");
+  return collect(ctx, "render batch", batch_timing(jobs, n));
 }
 
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {

@@ -1,0 +1,7 @@
+// lgpu_batch_k4.cu — batched render kernels for 4 hero wavelengths per path.
+#include "lgpu_render.cuh"
+
+namespace lgpu {
+template cudaError_t launch_batch_k<4>(const DevJob*, const uint64_t*, const uint32_t*, uint32_t, uint64_t,
+                                       uint64_t, bool, WaveState*, DevCounters*, cudaStream_t, KernelTimer*);
+}  // namespace lgpu

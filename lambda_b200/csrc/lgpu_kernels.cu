@@ -140,34 +140,23 @@ cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wav
   return cudaErrorInvalidValue;
 }
 
-uint32_t wave_samples(uint32_t npix, uint32_t spp) {
-  uint32_t const target = 1u << 21;
-  uint32_t s = (target + npix - 1) / npix;
-  if (s < 1) s = 1;
-  if (s > spp) s = spp;
-  return s;
-}
-
-namespace {
-__global__ void finalize_kernel(const float* __restrict__ film, uint32_t npix, uint32_t W, uint32_t H,
-                                float norm, float delta, float* __restrict__ out) {
-  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < npix; pix += gridDim.x * blockDim.x) {
-    uint32_t const i = pix / W, j = pix - i * W;
-    float const X = (film[3 * pix] / norm) * delta;
-    float const Y = (film[3 * pix + 1] / norm) * delta;
-    float const Z = (film[3 * pix + 2] / norm) * delta;
-    size_t const o = (size_t(H - i - 1) * W + j) * 3;
-    out[o + 0] = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
-    out[o + 1] = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
-    out[o + 2] = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
+cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* d_item_bases,
+                         const uint32_t* d_pix_bases, uint32_t n_jobs, uint64_t n_items,
+                         uint64_t chunk_items, bool linear, WaveState* wave, DevCounters* d_cnt,
+                         cudaStream_t st, KernelTimer* timer) {
+  if (n_jobs == 0 || n_items == 0) return cudaSuccess;
+  switch (hero_k) {
+    case 4:
+      return launch_batch_k<4>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
+                               d_cnt, st, timer);
+    case 8:
+      return launch_batch_k<8>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
+                               d_cnt, st, timer);
+    case 16:
+      return launch_batch_k<16>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
+                                d_cnt, st, timer);
   }
-}
-}  // namespace
-
-cudaError_t launch_finalize(const float* film, uint32_t npix, uint32_t W, uint32_t H, float norm,
-                            float delta, float* out, cudaStream_t st) {
-  finalize_kernel<<<(npix + 255) / 256, 256, 0, st>>>(film, npix, W, H, norm, delta, out);
-  return cudaGetLastError();
+  return cudaErrorInvalidValue;
 }
 
 uint32_t tonemap_partials_needed(uint64_t n_pixels) {

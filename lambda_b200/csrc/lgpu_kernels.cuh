@@ -25,7 +25,8 @@ struct PathBuf {
   uint64_t* rng;    // cap
   float* hero;      // cap
   uint32_t* depth;  // cap
-  uint32_t* item;   // cap: work item (sample * npix + pixel, relative to the chunk)
+  uint32_t* item;   // cap: work item, relative to the first item of the chunk
+  uint32_t* job;    // cap: job of the path (batched renders only)
   float* beta;      // K*cap
   float* acc;       // K*cap
 };
@@ -47,8 +48,9 @@ constexpr uint32_t kEndedBit = 0x80000000u;
 // Device buffers of the wavefront renderer; the context owns them.
 struct WaveState {
   uint32_t cap;        // queue capacity (paths in flight)
-  uint32_t npix;       // pixels of the frame
+  uint32_t npix;       // pixels of the frame (of all frames of a batch)
   uint32_t n_samples;  // samples per pixel in one chunk of the frame
+  uint64_t c0;         // first work item of the current chunk
   PathBuf in, out;     // current and next queue, swapped every iteration
   uint32_t* n_in;      // queue lengths (in ctl), swapped with the queues
   uint32_t* n_out;
@@ -56,13 +58,15 @@ struct WaveState {
   float* e_acc;        // K*cap: radiance of the paths ended this iteration
   float* e_hero;       // cap
   uint32_t* e_item;    // cap
+  uint32_t* e_job;     // cap (batched renders only)
   float* sray;         // 8*cap shadow rays (ox, oy, oz, dx, dy, dz, tmax, skip)
   uint32_t* s_target;  // cap: path of each shadow ray (`out` index, or ended index | kEndedBit)
   float* s_contrib;    // K*cap
+  uint32_t* s_job;     // cap (batched renders only)
   uint32_t* fb_queue;  // cap: `in` indices re-traced in the reference's object order
   uint32_t* ctl;       // kCtlWords counters
   uint32_t* h_ctl;     // pinned host copy of ctl
-  float* sbuf;         // 3 * npix * n_samples: XYZ of every (sample, pixel)
+  float* sbuf;         // 3 per work item of a chunk: XYZ of every (sample, pixel)
   float* film;         // 3*npix XYZ
 };
 
@@ -125,6 +129,83 @@ struct KernelTimer {
   }
 };
 
+// One job of a batched render: a scene, its settings and its place in
+// the batch.  Work items of the batch are numbered job after job; within a
+// job, item q is sample q / npix of pixel q % npix.
+struct DevJob {
+  DevScene S;
+  RenderArgs a;
+  uint64_t item_base;  // first work item of the job
+  uint32_t npix;
+  uint32_t pix_base;   // first pixel of the job in the batch film
+  float* out;          // linear RGB, width*height*3, row 0 at the top
+};
+
+#ifdef __CUDACC__
+// Job policies of the wavefront kernels.  OneJob (the plain renderer) keeps
+// its scene and settings in kernel parameters; JobTable (a batch) reads
+// them from a device table, and every path carries its job index.
+struct OneJob {
+  static constexpr bool kMulti = false;
+  DevScene S;
+  RenderArgs a;
+  uint32_t npix;
+  float* out;
+  __device__ __forceinline__ const DevScene& scene(uint32_t) const { return S; }
+  __device__ __forceinline__ const RenderArgs& args(uint32_t) const { return a; }
+  __device__ __forceinline__ uint32_t job_of_item(uint64_t) const { return 0; }
+  __device__ __forceinline__ uint32_t job_of_pixel(uint32_t) const { return 0; }
+  __device__ __forceinline__ uint64_t item_base(uint32_t) const { return 0; }
+  __device__ __forceinline__ uint32_t pix_base(uint32_t) const { return 0; }
+  __device__ __forceinline__ uint32_t npix_of(uint32_t) const { return npix; }
+  __device__ __forceinline__ float* out_of(uint32_t) const { return out; }
+};
+
+struct JobTable {
+  static constexpr bool kMulti = true;
+  const DevJob* d;
+  const uint64_t* item_bases;  // n + 1 entries, the last is the total
+  const uint32_t* pix_bases;   // n + 1 entries
+  uint32_t n;
+  __device__ __forceinline__ const DevScene& scene(uint32_t j) const { return d[j].S; }
+  __device__ __forceinline__ const RenderArgs& args(uint32_t j) const { return d[j].a; }
+  // the job whose range holds item g / pixel gp (binary search)
+  __device__ __forceinline__ uint32_t job_of_item(uint64_t g) const {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+      uint32_t const mid = (lo + hi + 1) >> 1;
+      if (item_bases[mid] <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ uint32_t job_of_pixel(uint32_t gp) const {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+      uint32_t const mid = (lo + hi + 1) >> 1;
+      if (pix_bases[mid] <= gp) lo = mid;
+      else hi = mid - 1;
+    }
+    return lo;
+  }
+  __device__ __forceinline__ uint64_t item_base(uint32_t j) const { return item_bases[j]; }
+  __device__ __forceinline__ uint32_t pix_base(uint32_t j) const { return pix_bases[j]; }
+  __device__ __forceinline__ uint32_t npix_of(uint32_t j) const { return d[j].npix; }
+  __device__ __forceinline__ float* out_of(uint32_t j) const { return d[j].out; }
+};
+#endif
+
+// Batched render of the jobs of `table` (n jobs, n_items work items,
+// n_pix pixels in all) with the wavefront kernels.
+cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* d_item_bases,
+                         const uint32_t* d_pix_bases, uint32_t n_jobs, uint64_t n_items,
+                         uint64_t chunk_items, bool linear, WaveState* wave, DevCounters* d_cnt,
+                         cudaStream_t st, KernelTimer* timer);
+template <int K>
+cudaError_t launch_batch_k(const DevJob* d_jobs, const uint64_t* d_item_bases, const uint32_t* d_pix_bases,
+                           uint32_t n_jobs, uint64_t n_items, uint64_t chunk_items, bool linear,
+                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+
 // Renders with the wavefront kernels when wave != nullptr, else with the
 // one-thread-per-pixel megakernel.  d_cnt points at 3 counter records:
 // everything, and with timer->on the closest-hit and shadow traversal apart.
@@ -133,16 +214,6 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
                             DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
                           DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
-
-// Samples per pixel in one wave for a frame of npix pixels: enough paths in
-// flight to fill the GPU (about 2^21), never more than spp.
-uint32_t wave_samples(uint32_t npix, uint32_t spp);
-
-// XYZ film (3 floats per pixel, scene row order) / norm * delta ->
-// linear BT.709 RGB in the reference's layout (row 0 at the top),
-// src/renderer.cpp:52-56.
-cudaError_t launch_finalize(const float* film, uint32_t npix, uint32_t W, uint32_t H, float norm,
-                            float delta, float* out, cudaStream_t st);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
 // doubles, at least tonemap_partials_needed(n)).

@@ -95,69 +95,60 @@ uint32_t persistent_blocks(F kernel, int threads, size_t smem) {
   return uint32_t(sms * per_sm);
 }
 
-template <int K>
-cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+// The streaming wavefront over n_items work items of `jobs`, in chunks of
+// at most chunk_items (the capacity of the (sample, pixel) film buffer).
+template <int K, class J>
+cudaError_t run_wave(const J& jobs, WaveState w, uint64_t n_items, uint64_t chunk_items, bool linear,
+                     DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
   DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
   DevCounters* const c_shadow = timer->on ? d_cnt + 2 : d_cnt;
-  if (!wave) {
-    uint32_t const blocks = (a.pixel_count + 127) / 128;
-    render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
-    timer->total++;
-    return cudaGetLastError();
-  }
-  WaveState w = *wave;
   size_t const smem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
   static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0, g_ptrace = 0, g_pshadow = 0,
                   g_fb = 0, g_fin = 0;
   if (!g_trace) {
-    cudaFuncSetAttribute(wf_trace, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    cudaFuncSetAttribute(wf_shadow<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-    cudaFuncSetAttribute(wf_trace_persistent<false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(wf_trace<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(wf_shadow<K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    cudaFuncSetAttribute(wf_trace_persistent<false, K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(smem));
-    cudaFuncSetAttribute(wf_trace_persistent<true, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(wf_trace_persistent<true, K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(smem));
-    g_trace = persistent_blocks(wf_trace, 128, smem);
-    g_shadow = persistent_blocks(wf_shadow<K>, 128, smem);
-    g_ptrace = persistent_blocks(wf_trace_persistent<false, K>, 128, smem);
-    g_pshadow = persistent_blocks(wf_trace_persistent<true, K>, 128, smem);
-    g_shade = persistent_blocks(wf_shade<K>, 128, 0);
-    g_gen = persistent_blocks(wf_generate_stream<K>, 256, 0);
-    g_fin = persistent_blocks(wf_finish<K>, 256, 0);
-    g_fb = persistent_blocks(wf_trace_fallback, 128, 0);
+    g_trace = persistent_blocks(wf_trace<J>, 128, smem);
+    g_shadow = persistent_blocks(wf_shadow<K, J>, 128, smem);
+    g_ptrace = persistent_blocks(wf_trace_persistent<false, K, J>, 128, smem);
+    g_pshadow = persistent_blocks(wf_trace_persistent<true, K, J>, 128, smem);
+    g_shade = persistent_blocks(wf_shade<K, J>, 128, 0);
+    g_gen = persistent_blocks(wf_generate_stream<K, J>, 256, 0);
+    g_fin = persistent_blocks(wf_finish<K, J>, 256, 0);
+    g_fb = persistent_blocks(wf_trace_fallback<J>, 128, 0);
   }
-  // the instance BVH kernels, or the reference's linear object loop
-  bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
   // Streaming: every iteration finishes the paths that ended in the last
   // one, appends new paths behind the queue up to its capacity (plan +
   // generate), then advances every queued path by one segment (trace,
-  // shade, shadow).  The frame's samples are processed in chunks of
-  // w.n_samples (the size of the (sample, pixel) film buffer).
-  uint32_t const chunk = w.n_samples;
-  for (uint32_t s0 = 0; s0 < a.spp && e == cudaSuccess; s0 += chunk) {
-    uint32_t const ns = (a.spp - s0 < chunk) ? (a.spp - s0) : chunk;
-    uint32_t const total = ns * w.npix;
+  // shade, shadow).
+  for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
+    uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
+    w.c0 = c0;
     wf_stream_init<<<1, 32, 0, st>>>(w);
     timer->total++;
     for (uint32_t it = 0;; it++) {
-      wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
+      wf_finish<K, J><<<g_fin, 256, 0, st>>>(jobs, w, d_cnt);
       wf_plan<<<1, 1, 0, st>>>(w, total);
-      wf_generate_stream<K><<<g_gen, 256, 0, st>>>(S, a, w, s0, d_cnt);
+      wf_generate_stream<K, J><<<g_gen, 256, 0, st>>>(jobs, w, d_cnt);
       timer->begin(0, st);
       if (linear) {
-        wf_trace<<<g_trace, 128, smem, st>>>(S, w, a.flags, c_closest);
+        wf_trace<J><<<g_trace, 128, smem, st>>>(jobs, w, c_closest);
       } else {
-        wf_trace_persistent<false, K><<<g_ptrace, 128, smem, st>>>(S, w, c_closest);
-        wf_trace_fallback<<<g_fb, 128, 0, st>>>(S, w, c_closest);
+        wf_trace_persistent<false, K, J><<<g_ptrace, 128, smem, st>>>(jobs, w, c_closest);
+        wf_trace_fallback<J><<<g_fb, 128, 0, st>>>(jobs, w, c_closest);
       }
       timer->end(0, st);
       timer->begin(2, st);
-      wf_shade<K><<<g_shade, 128, 0, st>>>(S, a, w, d_cnt);
+      wf_shade<K, J><<<g_shade, 128, 0, st>>>(jobs, w, d_cnt);
       timer->end(2, st);
       timer->begin(1, st);
-      if (linear) wf_shadow<K><<<g_shadow, 128, smem, st>>>(S, w, a.flags, c_shadow);
-      else wf_trace_persistent<true, K><<<g_pshadow, 128, smem, st>>>(S, w, c_shadow);
+      if (linear) wf_shadow<K, J><<<g_shadow, 128, smem, st>>>(jobs, w, c_shadow);
+      else wf_trace_persistent<true, K, J><<<g_pshadow, 128, smem, st>>>(jobs, w, c_shadow);
       timer->end(1, st);
       // finish, plan, generate, trace (+ fallback), shade, shadow
       timer->total += linear ? 6 : 7;
@@ -179,19 +170,45 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
       }
     }
     if (e != cudaSuccess) break;
-    wf_finish<K><<<g_fin, 256, 0, st>>>(S, w, d_cnt);
-    wf_reduce<<<(w.npix + 255) / 256, 256, 0, st>>>(w, ns);
+    wf_finish<K, J><<<g_fin, 256, 0, st>>>(jobs, w, d_cnt);
+    wf_reduce<J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w, c0 + total);
     timer->total += 2;
     e = cudaGetLastError();
   }
-  if (e == cudaSuccess) e = launch_finalize(w.film, w.npix, uint32_t(S.cam.width), uint32_t(S.cam.height),
-                                            float(a.spp) * float(K), S.lambda_delta, d_out, st);
-  timer->total++;
+  if (e == cudaSuccess) {
+    wf_finalize<K, J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w);
+    timer->total++;
+    e = cudaGetLastError();
+  }
   if (timer->on && e == cudaSuccess) {
     e = cudaStreamSynchronize(st);
     timer->harvest();
   }
   return e;
+}
+
+template <int K>
+cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
+                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+  if (!wave) {
+    uint32_t const blocks = (a.pixel_count + 127) / 128;
+    render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
+    timer->total++;
+    return cudaGetLastError();
+  }
+  OneJob const jobs{S, a, wave->npix, d_out};
+  // the instance BVH kernels, or the reference's linear object loop
+  bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
+  return run_wave<K>(jobs, *wave, uint64_t(wave->npix) * a.spp, uint64_t(wave->npix) * wave->n_samples,
+                     linear, d_cnt, st, timer);
+}
+
+template <int K>
+cudaError_t launch_batch_k(const DevJob* d_jobs, const uint64_t* d_item_bases, const uint32_t* d_pix_bases,
+                           uint32_t n_jobs, uint64_t n_items, uint64_t chunk_items, bool linear,
+                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+  JobTable const jobs{d_jobs, d_item_bases, d_pix_bases, n_jobs};
+  return run_wave<K>(jobs, *wave, n_items, chunk_items, linear, d_cnt, st, timer);
 }
 
 }  // namespace lgpu

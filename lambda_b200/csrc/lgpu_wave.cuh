@@ -114,24 +114,29 @@ __global__ void wf_plan(WaveState w, uint32_t total) {
 // Camera ray and hero wavelength as sample::camera and sample::spectrum
 // (cg.hpp:1534-1542, 1517-1531), random numbers drawn in the order of
 // Renderer::render (src/renderer.cpp:33-41).
-template <int K>
-__global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs a, WaveState w,
-                                                          uint32_t sample_base, DevCounters* cnt) {
+template <int K, class J>
+__global__ void __launch_bounds__(256) wf_generate_stream(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n_new = w.ctl[kCtlNew], first = w.ctl[kCtlFirst], pos = w.ctl[kCtlPos];
   uint32_t paths = 0;
-  float const omega = S.lambda_sup - S.lambda_inf;
-  const lgpu_camera& C = S.cam;
-  uint32_t const W = uint32_t(C.width);
   uint32_t const cap = w.cap;
   PathBuf const& in = w.in;
   for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n_new; k += gridDim.x * blockDim.x) {
     uint32_t const q = first + k;
-    uint32_t const s_local = q / w.npix;
-    uint32_t const pix = q - s_local * w.npix;
+    uint64_t const g = w.c0 + q;
+    uint32_t const jb = jobs.job_of_item(g);
+    const DevScene& S = jobs.scene(jb);
+    const RenderArgs& a = jobs.args(jb);
+    uint32_t const npix = jobs.npix_of(jb);
+    uint64_t const l = g - jobs.item_base(jb);
+    uint32_t const sample = uint32_t(l / npix);
+    uint32_t const pix = uint32_t(l - uint64_t(sample) * npix);
     uint32_t const p = pos + k;
+    float const omega = S.lambda_sup - S.lambda_inf;
+    const lgpu_camera& C = S.cam;
+    uint32_t const W = uint32_t(C.width);
     uint32_t const i = pix / W, j = pix - i * W;
     uint64_t rng = lgpu_path_state(a.seed, (uint64_t(a.stream_tag) << 32) | pix,
-                                   uint64_t(a.spp_offset) + sample_base + s_local);
+                                   uint64_t(a.spp_offset) + sample);
     float const u = float(j) + lgpu_flt(&rng);
     float const v = float(i) + lgpu_flt(&rng);
     f3 const Fx = f3{C.base_x[0], C.base_x[1], C.base_x[2]};
@@ -159,6 +164,7 @@ __global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs
     in.hero[p] = hero;
     in.depth[p] = 0;
     in.item[p] = q;
+    if (J::kMulti) in.job[p] = jb;
 #pragma unroll
     for (int kk = 0; kk < K; kk++) {
       in.beta[kk * cap + p] = 1.f;
@@ -172,15 +178,16 @@ __global__ void __launch_bounds__(256) wf_generate_stream(DevScene S, RenderArgs
 
 // Ended paths: radiance splatted to XYZ (addHeroλ(λ, Li/prob),
 // src/renderer.cpp:44) into the path's (sample, pixel) film entry.
-template <int K>
-__global__ void __launch_bounds__(256) wf_finish(DevScene S, WaveState w, DevCounters* cnt) {
+template <int K, class J>
+__global__ void __launch_bounds__(256) wf_finish(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = w.ctl[kCtlEnded];
-  float const omega = S.lambda_sup - S.lambda_inf;
-  float const step = omega / float(K);
-  float const prob_l = 1.f / omega;
   uint32_t const cap = w.cap;
   uint32_t nonfinite = 0;
   for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const DevScene& S = jobs.scene(J::kMulti ? w.e_job[e] : 0u);
+    float const omega = S.lambda_sup - S.lambda_inf;
+    float const step = omega / float(K);
+    float const prob_l = 1.f / omega;
     float const hero = w.e_hero[e];
     float sx = 0.f, sy = 0.f, sz = 0.f;
     bool finite = true;
@@ -200,19 +207,51 @@ __global__ void __launch_bounds__(256) wf_finish(DevScene S, WaveState w, DevCou
   flush_counters(cnt, 0u, 0u, ts, nonfinite);
 }
 
-// Film: per pixel, the (sample, pixel) entries summed in sample order.
-__global__ void __launch_bounds__(256) wf_reduce(WaveState w, uint32_t n_samples) {
-  for (uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x; pix < w.npix; pix += gridDim.x * blockDim.x) {
-    float X = w.film[3 * pix], Y = w.film[3 * pix + 1], Z = w.film[3 * pix + 2];
-    for (uint32_t s = 0; s < n_samples; s++) {
-      size_t const o = 3 * (size_t(s) * w.npix + pix);
+// Film: per pixel, the (sample, pixel) entries of the chunk [w.c0, c1)
+// added in sample order.
+template <class J>
+__global__ void __launch_bounds__(256) wf_reduce(J jobs, WaveState w, uint64_t c1) {
+  for (uint32_t gp = blockIdx.x * blockDim.x + threadIdx.x; gp < w.npix; gp += gridDim.x * blockDim.x) {
+    uint32_t const jb = jobs.job_of_pixel(gp);
+    uint32_t const npix = jobs.npix_of(jb);
+    uint64_t const base = jobs.item_base(jb) + (gp - jobs.pix_base(jb));
+    uint32_t const spp = jobs.args(jb).spp;
+    // samples s with w.c0 <= base + s * npix < c1
+    uint64_t const lo = w.c0 > base ? (w.c0 - base + npix - 1) / npix : 0;
+    uint64_t hi = c1 > base ? (c1 - base + npix - 1) / npix : 0;
+    if (hi > spp) hi = spp;
+    if (lo >= hi) continue;
+    float X = w.film[3 * size_t(gp)], Y = w.film[3 * size_t(gp) + 1], Z = w.film[3 * size_t(gp) + 2];
+    for (uint64_t s = lo; s < hi; s++) {
+      size_t const o = 3 * size_t(base + s * npix - w.c0);
       X += w.sbuf[o];
       Y += w.sbuf[o + 1];
       Z += w.sbuf[o + 2];
     }
-    w.film[3 * pix] = X;
-    w.film[3 * pix + 1] = Y;
-    w.film[3 * pix + 2] = Z;
+    w.film[3 * size_t(gp)] = X;
+    w.film[3 * size_t(gp) + 1] = Y;
+    w.film[3 * size_t(gp) + 2] = Z;
+  }
+}
+
+// XYZ film / (spp * K) * Δ -> linear BT.709 RGB in the reference's layout
+// (row 0 at the top), src/renderer.cpp:52-56, cg.hpp:144-148, 340-341.
+template <int K, class J>
+__global__ void __launch_bounds__(256) wf_finalize(J jobs, WaveState w) {
+  for (uint32_t gp = blockIdx.x * blockDim.x + threadIdx.x; gp < w.npix; gp += gridDim.x * blockDim.x) {
+    uint32_t const jb = jobs.job_of_pixel(gp);
+    const DevScene& S = jobs.scene(jb);
+    uint32_t const pix = gp - jobs.pix_base(jb);
+    uint32_t const W = uint32_t(S.cam.width), H = uint32_t(S.cam.height);
+    uint32_t const i = pix / W, j = pix - i * W;
+    float const norm = float(jobs.args(jb).spp) * float(K);
+    float const X = (w.film[3 * size_t(gp)] / norm) * S.lambda_delta;
+    float const Y = (w.film[3 * size_t(gp) + 1] / norm) * S.lambda_delta;
+    float const Z = (w.film[3 * size_t(gp) + 2] / norm) * S.lambda_delta;
+    float* out = jobs.out_of(jb) + (size_t(H - i - 1) * W + j) * 3;
+    out[0] = 3.2404542f * X - 1.5371385f * Y - 0.4985314f * Z;
+    out[1] = -0.9692660f * X + 1.8760108f * Y + 0.0415560f * Z;
+    out[2] = 0.0556434f * X - 0.2040259f * Y + 1.0572252f * Z;
   }
 }
 
@@ -220,7 +259,8 @@ __global__ void __launch_bounds__(256) wf_reduce(WaveState w, uint32_t n_samples
 
 // Closest hit of every queued path with one thread per ray (the reference's
 // linear object loop, or the instance BVH).
-__global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
+template <class J>
+__global__ void __launch_bounds__(128) wf_trace(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   StackEntry lstack[kStackCap];
@@ -228,9 +268,11 @@ __global__ void __launch_bounds__(128) wf_trace(DevScene S, WaveState w, uint32_
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
-  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
   uint32_t const n = *w.n_in;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t const jb = J::kMulti ? w.in.job[i] : 0u;
+    const DevScene& S = jobs.scene(jb);
+    bool const ref_order = (jobs.args(jb).flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
     Ray const r = load_ray(w.in.ray, w.cap, i);
     HitRec h;
     clear_hit(h, kFltMax);
@@ -260,8 +302,8 @@ __device__ __forceinline__ void add_shadow(const WaveState& w, uint32_t s) {
 // per warp once kRefill of them are waiting.
 constexpr int kRefill = 8;
 
-template <bool ANY, int K>
-__global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveState w, DevCounters* cnt) {
+template <bool ANY, int K, class J>
+__global__ void __launch_bounds__(128, 6) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
@@ -274,7 +316,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
   int const lane = threadIdx.x & 31;
   TraceState t;
   bool active = false, exhausted = false;
-  uint32_t idx = 0, wobj = 0;
+  uint32_t idx = 0, wobj = 0, jb = 0;
   int phase = 1;
   while (true) {
     unsigned const idle = __ballot_sync(FULL, !active);
@@ -288,6 +330,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
         uint32_t const my = base + uint32_t(__popc(idle & ((1u << lane) - 1u)));
         if (my < n) {
           idx = my;
+          if (J::kMulti) jb = ANY ? w.s_job[my] : w.in.job[my];
           if (ANY) {
             t.w = load_ray(w.sray, cap, my);
             clear_hit(t.h, w.sray[6 * cap + my]);
@@ -300,7 +343,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
           t.any = ANY;
           t.ilimit = UINT32_MAX;
           phase = 1;
-          trace_begin(S, t, st);
+          trace_begin(jobs.scene(jb), t, st);
           active = true;
           rays++;
         }
@@ -310,7 +353,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
       if (exhausted) break;
       continue;
     }
-    if (active && trace_step<ANY>(S, t, st, ts)) {
+    if (active && trace_step<ANY>(jobs.scene(jb), t, st, ts)) {
       active = false;
       if (ANY) {
         if (!t.hit_any) add_shadow<K>(w, idx);
@@ -327,7 +370,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
           t.skip = wobj;
           t.ilimit = UINT32_MAX;
           phase = 3;
-          trace_begin(S, t, st);
+          trace_begin(jobs.scene(jb), t, st);
           active = true;
         }
         continue;
@@ -352,7 +395,7 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
         t.skip = UINT32_MAX;
         t.ilimit = wobj;
         phase = 2;
-        trace_begin(S, t, st);
+        trace_begin(jobs.scene(jb), t, st);
         active = true;
         continue;
       }
@@ -364,13 +407,15 @@ __global__ void __launch_bounds__(128, 6) wf_trace_persistent(DevScene S, WaveSt
 
 // Extension rays whose closest hit depends on the reference's object order
 // (see scene_hit): the linear object loop.
-__global__ void __launch_bounds__(128) wf_trace_fallback(DevScene S, WaveState w, DevCounters* cnt) {
+template <class J>
+__global__ void __launch_bounds__(128) wf_trace_fallback(J jobs, WaveState w, DevCounters* cnt) {
   StackEntry lstack[kStackCap];
   StackEntry ltstack[kTlasStackCap];
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t const n = w.ctl[kCtlFallback];
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     uint32_t const p = w.fb_queue[i];
+    const DevScene& S = jobs.scene(J::kMulti ? w.in.job[p] : 0u);
     Ray const r = load_ray(w.in.ray, w.cap, p);
     HitRec h;
     clear_hit(h, kFltMax);
@@ -388,18 +433,21 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(DevScene S, WaveState w
 // queued path: emitter hit (73-84), light importance sample with the MIS
 // power heuristic (87-113, its visibility left to the shadow kernel),
 // material importance sample with Russian roulette (115-143).
-template <int K>
-__global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveState w, DevCounters* cnt) {
+template <int K, class J>
+__global__ void __launch_bounds__(128) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
-  float const omega = S.lambda_sup - S.lambda_inf;
-  float const step = omega / float(K);
   PathBuf const& in = w.in;
   PathBuf const& out = w.out;
   enum : int { kEnd = 0, kEmit = 1, kScatter = 2 };
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     uint32_t const i = base + threadIdx.x;
     bool const live = i < n;
+    uint32_t const jb = (J::kMulti && live) ? in.job[i] : 0u;
+    const DevScene& S = jobs.scene(jb);
+    const RenderArgs& a = jobs.args(jb);
+    float const omega = S.lambda_sup - S.lambda_inf;
+    float const step = omega / float(K);
     int kind = kEnd;
     bool cont = false, shadow = false, needs_test = false;
     f3 sp = f3{0.f, 0.f, 0.f}, sd = f3{0.f, 0.f, 1.f};
@@ -514,12 +562,15 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
       out.hero[o_pos] = hero;
       out.depth[o_pos] = in.depth[i] + 1;
       out.item[o_pos] = in.item[i];
+      if (J::kMulti) out.job[o_pos] = jb;
     } else {
       w.e_hero[e_pos] = hero;
       w.e_item[e_pos] = in.item[i];
+      if (J::kMulti) w.e_job[e_pos] = jb;
     }
     if (shadow) {
       w.s_target[s_pos] = cont ? o_pos : (e_pos | kEndedBit);
+      if (J::kMulti) w.s_job[s_pos] = jb;
       w.sray[0 * cap + s_pos] = sp.x;
       w.sray[1 * cap + s_pos] = sp.y;
       w.sray[2 * cap + s_pos] = sp.z;
@@ -536,8 +587,8 @@ __global__ void __launch_bounds__(128) wf_shade(DevScene S, RenderArgs a, WaveSt
 // ---- shadow -----------------------------------------------------------------------
 
 // Any-hit test of every shadow ray with one thread per ray.
-template <int K>
-__global__ void __launch_bounds__(128) wf_shadow(DevScene S, WaveState w, uint32_t flags, DevCounters* cnt) {
+template <int K, class J>
+__global__ void __launch_bounds__(128) wf_shadow(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   StackEntry lstack[kStackCap];
@@ -545,10 +596,12 @@ __global__ void __launch_bounds__(128) wf_shadow(DevScene S, WaveState w, uint32
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
-  bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
   uint32_t const n = w.ctl[kCtlShadow];
   uint32_t const cap = w.cap;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    uint32_t const jb = J::kMulti ? w.s_job[i] : 0u;
+    const DevScene& S = jobs.scene(jb);
+    bool const ref_order = (jobs.args(jb).flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
     Ray const r = load_ray(w.sray, cap, i);
     HitRec h;
     clear_hit(h, w.sray[6 * cap + i]);

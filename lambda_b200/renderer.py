@@ -65,6 +65,52 @@ class Context:
         self._scene_id = id(scene)
         return flat
 
+    def upload_many(self, scenes):
+        """Scene table for batched renders: scene k goes to slot k (slot 0
+        is also the scene of render/trace)."""
+        flats = [s if isinstance(s, FlatScene) else FlatScene(s) for s in scenes]
+        arr = (ctypes.POINTER(L.Scene) * len(flats))(*[f.ptr() for f in flats])
+        L.check(self.h, self._lib.lgpu_upload_scenes(self.h, arr, len(flats)), "upload_scenes")
+        self.flat = flats[0]
+        self.flats = flats
+        self._scene_id = None
+        return flats
+
+    def slot_size(self, slot):
+        c = self.flats[slot].scene.cam
+        return int(c.width), int(c.height)
+
+    @staticmethod
+    def _jobs(jobs, outs):
+        arr = (L.Job * len(jobs))()
+        for k, (j, o) in enumerate(zip(jobs, outs)):
+            arr[k].scene = int(j["scene"])
+            arr[k].params = L.RenderParams(spp=int(j["spp"]), max_scatterings=int(j["max_scatterings"]),
+                                           sample_p=float(j["sample_p"]), flags=int(j.get("flags", 0)),
+                                           seed=int(j.get("seed", 0)),
+                                           spp_offset=int(j.get("spp_offset", 0)))
+            arr[k].out = o
+        return arr
+
+    def render_batch(self, jobs):
+        """Renders every job (dicts: scene, spp, max_scatterings, sample_p
+        and optionally seed, flags, spp_offset) in one batched launch;
+        returns one (height, width, 3) image per job."""
+        imgs = []
+        for j in jobs:
+            w, h = self.slot_size(j["scene"])
+            imgs.append(np.empty((h, w, 3), np.float32))
+        arr = self._jobs(jobs, [im.ctypes.data for im in imgs])
+        L.check(self.h, self._lib.lgpu_render_batch(self.h, arr, len(jobs)), "render_batch")
+        return imgs
+
+    def render_batch_device(self, jobs, d_outs, stream=None):
+        """render_batch with device outputs (pointers, one per job)."""
+        arr = self._jobs(jobs, d_outs)
+        L.check(self.h, self._lib.lgpu_render_batch_device(self.h, arr, len(jobs),
+                                                           ctypes.c_void_p(stream or 0)),
+                "render_batch_device")
+
     @property
     def size(self):
         c = self.flat.scene.cam

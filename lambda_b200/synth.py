@@ -398,3 +398,68 @@ def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 
     with open(path, "w") as f:
         json.dump(scene, f, indent=1)
     return path
+
+
+def batch_job(out_dir, n_instances, subdiv, mesh_dir, seed, width):
+    """A batched-render job scene: the box room with n_instances copies of a
+    displaced icosphere (subdivision subdiv, shared by every job through
+    mesh_dir) standing on its floor, materials drawn as in instanced();
+    returns the .nls path."""
+    base = box_room(out_dir, width=width)
+    d = os.path.abspath(out_dir)
+    os.makedirs(mesh_dir, exist_ok=True)
+    mesh_path = os.path.join(os.path.abspath(mesh_dir), f"icosphere_s{subdiv}.obj")
+    if not os.path.exists(mesh_path):
+        V, N, F = displaced_icosphere(subdiv, 1234)
+        write_indexed_obj(mesh_path, V, N, F)
+    with open(base) as f:
+        scene = json.load(f)
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(np.sqrt(n_instances)))
+    spacing = 0.9 / side
+    s = 0.4 * spacing
+    for i in range(n_instances):
+        kind = ["lambertian", "blinn", "thinfilm"][int(rng.integers(0, 3))]
+        name = f"m{i}"
+        if kind == "lambertian":
+            p = os.path.join(d, f"albedo_{i}.csv")
+            smooth_random_csv(p, rng)
+            scene["materials"].append({"name": name, "type": "lambertian", "albedo": {"val": p}})
+        elif kind == "blinn":
+            p = os.path.join(d, f"kd_{i}.csv")
+            smooth_random_csv(p, rng, 0.05, 0.6)
+            alpha = 2 * int(round(np.exp(rng.uniform(np.log(8), np.log(2048))) / 2))
+            scene["materials"].append({"name": name, "type": "blinn", "Kd": {"val": p},
+                                       "Ks": {"val": float(rng.uniform(0.2, 0.5))}, "glossiness": alpha})
+        else:
+            alpha = 2 * int(round(np.exp(rng.uniform(np.log(8), np.log(2048))) / 2))
+            scene["materials"].append({"name": name, "type": "thinfilm",
+                                       "film_ior": {"val": float(rng.uniform(1.33, 1.6))},
+                                       "base_ior": {"val": 1.5}, "glossiness": alpha,
+                                       "thickness": float(rng.uniform(200, 800))})
+        gx, gy = i % side, i // side
+        scene["objects"].append({"name": f"inst{i}", "type": "trimesh", "material": name,
+                                 "source": mesh_path,
+                                 "transform": {"scale": [s, s, s],
+                                               "rotate": {"axis": [0, 0, 1],
+                                                          "degrees": float(rng.uniform(0, 360))},
+                                               "translate": [0.05 + (gx + 0.5) * spacing,
+                                                             0.05 + (gy + 0.5) * spacing, s]}})
+    with open(base, "w") as f:
+        json.dump(scene, f, indent=1)
+    return base
+
+
+def batch_jobs(n_jobs=64, seed=2024):
+    """The batched workload: per job an instance count U[1,128], an
+    icosphere subdivision from {5, 6, 7} (20K-328K triangles per instance),
+    a square resolution from {128, 256, 512, 1024}, spp log-uniform in
+    [4, 256] and bounces U[4, 32]; p = 0.8.  Returns a list of dicts."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n_jobs):
+        jobs.append(dict(n_instances=int(rng.integers(1, 129)), subdiv=int(rng.integers(5, 8)),
+                         width=int(rng.choice([128, 256, 512, 1024])),
+                         spp=int(round(np.exp(rng.uniform(np.log(4), np.log(256))))),
+                         max_scatterings=int(rng.integers(4, 33)), sample_p=0.8, seed=1000 + k))
+    return jobs
