@@ -129,15 +129,15 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profile_traffic_per_launch(kind):
-    """DRAM bytes (read + write) per launch of kernel kind (0 closest-hit,
-    1 shadow, 2 shading) on the full workload, from the committed ncu
-    summary profiles/traffic_instanced.json, or None."""
+def profile_traffic_per_ray(kind):
+    """DRAM bytes (read + write) per ray of kernel kind (0 closest-hit,
+    1 shadow) from the committed ncu summary
+    profiles/traffic_instanced.json, or None."""
     p = os.path.join(REPO, "profiles", "traffic_instanced.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return float(d["dram_bytes_per_launch"][str(kind)])
+        return float(d["dram_bytes_per_ray"][str(kind)])
     except (OSError, KeyError, ValueError, TypeError):
         return None
 
@@ -174,7 +174,8 @@ def kernel_roofline(ctx, spp, B, p, stream):
                 k["inst_tests"] * BYTES_PER_INST + k["rays"] * BYTES_PER_RAY)
         achieved = algo / (k["ms"] / 1e3) / 1e9
     launches = max(int(k["launches"]), 1)
-    tpl = profile_traffic_per_launch(top)
+    tpr = profile_traffic_per_ray(top)
+    tpl = tpr * k["rays"] / launches if tpr is not None else None
     return {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": (achieved / peak) if achieved is not None else None,
             "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"

@@ -291,6 +291,29 @@ typedef struct lgpu_job {
 int lgpu_render_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n);
 int lgpu_render_batch_device(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, void* stream);
 
+/* Gradients of an image loss with respect to material parameters by path
+   replay (no counterpart in the reference, which renders only; this is the
+   adjoint of Renderer::tracePath, src/renderer.cpp:64-146).  Given
+   dloss_dimage = dLoss/d(linear RGB) (cam.width*cam.height*3 floats, the
+   lgpu_render layout), renders slot 0 with `params` and writes
+     grad_spectra   n_spectra*n_bins floats: dLoss/d(bin) of every
+                    spectrum of the uploaded table (lgpu_scene.spectra) used
+                    as a Lambertian albedo or a thin-film IOR (0 elsewhere);
+     grad_materials n_materials*4 floats per material: [0] dLoss/d thin-film
+                    thickness (nm), [1] dLoss/d lobe exponent α (Blinn and
+                    thin film), [2..3] 0;
+     out_linrgb     the primal image of the same paths (may be NULL).
+   Sampling decisions and MIS weights are held fixed (detached), so the
+   estimate is unbiased for the gradient of the expected loss.  Paths are
+   recomputed from their random streams; nothing per vertex is stored.
+   max_scatterings <= 62.  lgpu_adjoint: host buffers; lgpu_adjoint_device:
+   device buffers, on `stream` (NULL: the context's stream). */
+int lgpu_adjoint(lgpu_ctx* ctx, const lgpu_render_params* params, const float* dloss_dimage,
+                 float* grad_spectra, float* grad_materials, float* out_linrgb);
+int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const float* d_dloss_dimage,
+                        float* d_grad_spectra, float* d_grad_materials, float* d_out_linrgb,
+                        void* stream);
+
 /* intersect::scene (cg.hpp:1469-1489) on n rays given as 6 floats each
    (origin xyz, direction xyz) in host memory; writes n lgpu_hit. */
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,

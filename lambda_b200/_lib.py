@@ -136,6 +136,8 @@ SIGNATURES = {
     "lgpu_render_batch_device": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, _vp]),
     "lgpu_render": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp]),
     "lgpu_render_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp]),
+    "lgpu_adjoint": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp, _vp, _vp]),
+    "lgpu_adjoint_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp, _vp, _vp, _vp]),
     "lgpu_trace_closest": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),
     "lgpu_tonemap": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                     _vp, _vp]),

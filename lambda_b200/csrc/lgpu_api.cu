@@ -72,6 +72,7 @@ struct lgpu_ctx {
   DevArray<uint64_t> job_items;
   DevArray<uint32_t> job_pixels;
   DevArray<float> batch_out;
+  DevArray<float> adj_buf;
   // working buffers
   DevArray<float> out;
   // wavefront state (lgpu_wave.cuh), sized for the largest frame rendered
@@ -193,7 +194,7 @@ struct Carver {
 // wavelengths, npix pixels and a chunk of sbuf_items work items; with
 // base == nullptr it only counts the bytes.
 size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint64_t sbuf_items, bool batch,
-                   WaveState& ws) {
+                   bool adjoint, WaveState& ws) {
   Carver c{base};
   size_t const n = cap;
   for (PathBuf* pb : {&ws.in, &ws.out}) {
@@ -205,6 +206,7 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
     pb->job = batch ? c.take<uint32_t>(n) : nullptr;
     pb->beta = c.take<float>(size_t(K) * n);
     pb->acc = c.take<float>(size_t(K) * n);
+    pb->gw = adjoint ? c.take<float>(size_t(K) * n) : nullptr;
   }
   ws.hit = c.take<float>(9 * n);
   ws.e_acc = c.take<float>(size_t(K) * n);
@@ -219,6 +221,10 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
   ws.ctl = c.take<uint32_t>(kCtlWords);
   ws.film = c.take<float>(3 * size_t(npix));
   ws.sbuf = c.take<float>(3 * size_t(sbuf_items));
+  ws.ltot = adjoint ? c.take<float>(size_t(K) * sbuf_items) : nullptr;
+  ws.vis = adjoint ? c.take<uint64_t>(sbuf_items) : nullptr;
+  ws.s_item = adjoint ? c.take<uint32_t>(n) : nullptr;
+  ws.s_depth = adjoint ? c.take<uint32_t>(n) : nullptr;
   return c.off;
 }
 
@@ -230,13 +236,13 @@ constexpr uint64_t kSbufBytes = uint64_t(1) << 31;
 // Sizes the wavefront buffers for npix pixels, n_items work items in chunks
 // of chunk_items, and fills ws.
 int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint64_t n_items, uint64_t chunk_items, bool batch,
-                WaveState& ws) {
+                WaveState& ws, bool adjoint = false) {
   uint32_t const K = ctx->S.hero_k;
   uint32_t const cap = uint32_t(n_items < kQueueCap ? n_items : kQueueCap);
-  size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, ws);
+  size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, adjoint, ws);
   cudaError_t const e = ensure(ctx->w_arena, bytes);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront buffers");
-  wave_layout(ctx->w_arena.ptr, cap, K, npix, chunk_items, batch, ws);
+  wave_layout(ctx->w_arena.ptr, cap, K, npix, chunk_items, batch, adjoint, ws);
   ws.cap = cap;
   ws.npix = npix;
   ws.n_samples = 0;
@@ -368,6 +374,39 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
   return LGPU_OK;
 }
 
+// Path-replay adjoint of a render of slot 0 (lgpu_adjoint.cuh).
+int adjoint_impl(lgpu_ctx* ctx, const lgpu_render_params* p, const float* d_dimg, float* d_gspec, float* d_gmat,
+                 float* d_img, cudaStream_t st) {
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  if (p->max_scatterings > 62)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "the adjoint records visibility for at most 63 vertices "
+                                                "(max_scatterings <= 62)");
+  if (p->flags & LGPU_FLAG_MEGAKERNEL)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "the adjoint runs on the wavefront kernels only");
+  const DevScene& S = ctx->S;
+  RenderArgs const a = render_args(p, S);
+  uint64_t const npix = a.pixel_count;
+  uint64_t const n_items = npix * a.spp;
+  // per work item of a chunk: 12 B film entry, 4K B radiance, 8 B visibility
+  uint64_t const per_item = 12 + 4ull * S.hero_k + 8;
+  uint64_t const max_items = (uint64_t(1) << 32) / per_item;
+  uint64_t const chunk = n_items < max_items ? n_items : max_items;
+  WaveState ws{};
+  if (int r = ensure_wave(ctx, a.pixel_count, n_items, chunk, false, ws, true)) return r;
+  if (int r = prepare_timer(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) != 0)) return r;
+  size_t const n_spec = ctx->slots[0].spectra.n;
+  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_gspec, 0, n_spec * sizeof(float), st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_gmat, 0, 4 * size_t(S.n_materials) * sizeof(float), st);
+  AdjointArgs const g{d_dimg, d_gspec, d_gmat};
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
+  if (e == cudaSuccess) e = launch_adjoint(S.hero_k, S, a, &ws, chunk, d_img, g, ctx->counters, st, &ctx->timer);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
+  return LGPU_OK;
+}
+
 bool batch_timing(const lgpu_job* jobs, uint32_t n) {
   for (uint32_t k = 0; k < n; k++)
     if ((jobs[k].params.flags & LGPU_FLAG_KERNEL_TIMING) && !(n == 1 && (jobs[k].params.flags & LGPU_FLAG_MEGAKERNEL)))
@@ -472,6 +511,11 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   ctx->release_scene();
   ctx->out.release();
   ctx->w_arena.release();
+  ctx->jobs.release();
+  ctx->job_items.release();
+  ctx->job_pixels.release();
+  ctx->batch_out.release();
+  ctx->adj_buf.release();
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   ctx->rays.release();
   ctx->hits.release();
@@ -590,6 +634,48 @@ int lgpu_render_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n) {
                         ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch readback");
   return collect(ctx, "render batch", batch_timing(jobs, n));
+}
+
+int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const float* d_dloss_dimage,
+                        float* d_grad_spectra, float* d_grad_materials, float* d_out_linrgb, void* stream) {
+  if (!ctx || !params || !d_dloss_dimage || !d_grad_spectra || !d_grad_materials)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  int const rc = adjoint_impl(ctx, params, d_dloss_dimage, d_grad_spectra, d_grad_materials, d_out_linrgb, st);
+  if (rc != LGPU_OK) return rc;
+  cudaError_t const e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint");
+  return collect(ctx, "adjoint", (params->flags & LGPU_FLAG_KERNEL_TIMING) != 0);
+}
+
+int lgpu_adjoint(lgpu_ctx* ctx, const lgpu_render_params* params, const float* dloss_dimage, float* grad_spectra,
+                 float* grad_materials, float* out_linrgb) {
+  if (!ctx || !params || !dloss_dimage || !grad_spectra || !grad_materials)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  size_t const npx = size_t(ctx->S.cam.width) * ctx->S.cam.height * 3;
+  size_t const n_spec = ctx->slots[0].spectra.n;
+  size_t const n_mat = 4 * size_t(ctx->S.n_materials);
+  // one device buffer: dLoss/dimage, image, spectral and material gradients
+  cudaError_t e = ensure(ctx->adj_buf, 2 * npx + n_spec + n_mat);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint buffers");
+  float* const d_dimg = ctx->adj_buf.ptr;
+  float* const d_img = d_dimg + npx;
+  float* const d_gs = d_img + npx;
+  float* const d_gm = d_gs + n_spec;
+  cudaStream_t const st = ctx->stream;
+  e = cudaMemcpyAsync(d_dimg, dloss_dimage, npx * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint upload");
+  int const rc = adjoint_impl(ctx, params, d_dimg, d_gs, d_gm, out_linrgb ? d_img : nullptr, st);
+  if (rc != LGPU_OK) return rc;
+  e = cudaMemcpyAsync(grad_spectra, d_gs, n_spec * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(grad_materials, d_gm, n_mat * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && out_linrgb)
+    e = cudaMemcpyAsync(out_linrgb, d_img, npx * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint readback");
+  return collect(ctx, "adjoint", (params->flags & LGPU_FLAG_KERNEL_TIMING) != 0);
 }
 
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {

@@ -159,6 +159,17 @@ cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* 
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_adjoint(uint32_t hero_k, const DevScene& S, const RenderArgs& a, WaveState* wave,
+                           uint64_t chunk_items, float* d_img, const AdjointArgs& g, DevCounters* d_cnt,
+                           cudaStream_t st, KernelTimer* timer) {
+  switch (hero_k) {
+    case 4: return launch_adjoint_k<4>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
+    case 8: return launch_adjoint_k<8>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
+    case 16: return launch_adjoint_k<16>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
+  }
+  return cudaErrorInvalidValue;
+}
+
 uint32_t tonemap_partials_needed(uint64_t n_pixels) {
   uint64_t const b = (n_pixels + kTmThreads - 1) / kTmThreads;
   return uint32_t(b < kTmMaxBlocks ? (b ? b : 1) : kTmMaxBlocks);

@@ -28,7 +28,8 @@ struct PathBuf {
   uint32_t* item;   // cap: work item, relative to the first item of the chunk
   uint32_t* job;    // cap: job of the path (batched renders only)
   float* beta;      // K*cap
-  float* acc;       // K*cap
+  float* acc;       // K*cap (path replay: the radiance still to come)
+  float* gw;        // K*cap, path replay: dL/d(radiance) per hero wavelength
 };
 
 // Counters of the wavefront renderer (WaveState::ctl).
@@ -68,6 +69,13 @@ struct WaveState {
   uint32_t* h_ctl;     // pinned host copy of ctl
   float* sbuf;         // 3 per work item of a chunk: XYZ of every (sample, pixel)
   float* film;         // 3*npix XYZ
+  // path replay (lgpu_adjoint): the primal pass records every path's
+  // radiance and which of its shadow rays were unoccluded; the replay
+  // pass reads them back
+  float* ltot;         // K per work item of the chunk, or nullptr
+  uint64_t* vis;       // per work item: bit v set = the shadow ray of vertex v reached its light
+  uint32_t* s_item;    // cap: work item of each shadow ray
+  uint32_t* s_depth;   // cap: its vertex
 };
 
 struct RenderArgs {
@@ -214,6 +222,21 @@ cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* w
                             DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
                           DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+
+// Path-replay adjoint (lgpu_adjoint.cuh): primal image (d_img, may be null)
+// and gradients of the loss whose image gradient is dimg.
+struct AdjointArgs {
+  const float* dimg;  // dLoss/d(linear RGB), width*height*3, row 0 at the top
+  float* g_spec;      // n_spectra * n_bins
+  float* g_mat;       // n_materials * 4: thickness, alpha, 0, 0
+};
+cudaError_t launch_adjoint(uint32_t hero_k, const DevScene& S, const RenderArgs& a, WaveState* wave,
+                           uint64_t chunk_items, float* d_img, const AdjointArgs& g, DevCounters* d_cnt,
+                           cudaStream_t st, KernelTimer* timer);
+template <int K>
+cudaError_t launch_adjoint_k(const DevScene& S, const RenderArgs& a, WaveState* wave, uint64_t chunk_items,
+                             float* d_img, const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st,
+                             KernelTimer* timer);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
 // doubles, at least tonemap_partials_needed(n)).

@@ -303,13 +303,14 @@ struct BsdfScalars {
   float a;     // lambertian/blinn: max(0, cos_i); thinfilm: cos_i (i·h)
   float b;     // blinn: pow(1-cos_o, 5); thinfilm: pow(1-cos_i, 5)
   float c;     // blinn: pow(h·n, α) or pow(|ht·n|, α); thinfilm: pow(h·n, α)
+  float lnhn;  // log of the |cosine| raised to α in c (for d/dα)
 };
 
 __device__ __forceinline__ BsdfScalars bsdf_scalars(const DevScene& S, const DevMaterial& m,
                                                     float x0, f3 i, f3 o, f3 n, bool front) {
   BsdfScalars r;
   r.kind = 0;
-  r.a = r.b = r.c = 0.f;
+  r.a = r.b = r.c = r.lnhn = 0.f;
   if (m.type == LGPU_MAT_LAMBERTIAN) {  // cg.hpp:921-926
     r.kind = 1;
     r.a = fmax0(fdot(i, n));
@@ -320,13 +321,17 @@ __device__ __forceinline__ BsdfScalars bsdf_scalars(const DevScene& S, const Dev
     if (cos_i * cos_o > 0.f) {
       r.kind = 2;
       f3 const h = half_vec(i, o, n);
-      r.c = powf(fdot(h, n), m.alpha);
+      float const hn = fdot(h, n);
+      r.c = powf(hn, m.alpha);
+      r.lnhn = logf(fabsf(hn));
     } else {
       r.kind = 3;
       float const ior0 = spec_at(S, m.spectrum[4], x0);
       float const eta0 = front ? 1.f / ior0 : ior0;
       f3 const ht = fnorm(f3{i.x + eta0 * o.x, i.y + eta0 * o.y, i.z + eta0 * o.z});
-      r.c = powf(fabsf(fdot(ht, n)), m.alpha);
+      float const hn = fabsf(fdot(ht, n));
+      r.c = powf(hn, m.alpha);
+      r.lnhn = logf(hn);
     }
   } else if (m.type == LGPU_MAT_THINFILM) {  // cg.hpp:1032-1051
     if (front && !(fdot(i, n) < 0.f) && !(fdot(o, n) < 0.f)) {
@@ -334,7 +339,9 @@ __device__ __forceinline__ BsdfScalars bsdf_scalars(const DevScene& S, const Dev
       f3 const h = half_vec(i, o, n);
       r.a = fdot(i, h);
       r.b = powf(1.f - r.a, 5.f);
-      r.c = powf(fdot(h, n), m.alpha);
+      float const hn = fdot(h, n);
+      r.c = powf(hn, m.alpha);
+      r.lnhn = logf(fabsf(hn));
     }
   }
   return r;
@@ -392,6 +399,7 @@ struct MatSample {
   int lobe;  // 1 lambert/blinn-diffuse (a=max(0,cos)), 2 blinn reflect, 3 blinn transmit, 4 thinfilm
   float a, b, c;
   float cos_oh;  // blinn: o·h, for the per-wavelength total-internal-reflection test
+  float lnhn;    // log of the |cosine| raised to α in c (for d/dα)
 };
 
 __device__ __forceinline__ MatSample sample_material(const DevScene& S, const DevMaterial& m, float x0,
@@ -400,7 +408,7 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
   ms.ok = false;
   ms.prob = 0.f;
   ms.lobe = 0;
-  ms.a = ms.b = ms.c = ms.cos_oh = 0.f;
+  ms.a = ms.b = ms.c = ms.cos_oh = ms.lnhn = 0.f;
   ms.dir = f3{0.f, 0.f, 1.f};
   f3 const n = H.front ? H.F.z : neg3(H.F.z);
   if (m.type == LGPU_MAT_LAMBERTIAN) {  // cg.hpp:1755-1777
@@ -454,6 +462,7 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
       ms.ok = true;
       ms.cos_oh = cos_oh;
       ms.c = powf(w.z, m.alpha);
+      ms.lnhn = logf(fabsf(w.z));
       if (lobe < pp_spec * p_r) {
         ms.prob = pp_spec * p_r * hp * 0.25f;
         ms.dir = reflect(o, h);
@@ -497,7 +506,9 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
       f3 const hh = half_vec(i, o, nz);
       ms.a = fdot(i, hh);
       ms.b = powf(1.f - ms.a, 5.f);
-      ms.c = powf(fdot(hh, nz), m.alpha);
+      float const hn = fdot(hh, nz);
+      ms.c = powf(hn, m.alpha);
+      ms.lnhn = logf(fabsf(hn));
     }
     return ms;
   }

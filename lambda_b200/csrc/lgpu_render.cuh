@@ -95,95 +95,137 @@ uint32_t persistent_blocks(F kernel, int threads, size_t smem) {
   return uint32_t(sms * per_sm);
 }
 
-// The streaming wavefront over n_items work items of `jobs`, in chunks of
-// at most chunk_items (the capacity of the (sample, pixel) film buffer).
+// Launch grids of the wavefront kernels: every SM filled to the kernel's
+// occupancy limit (computed once per instantiation).
+struct WaveGrids {
+  uint32_t trace, shade, shadow, gen, ptrace, pshadow, fb, fin;
+};
+constexpr size_t kTraceSmem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
+
 template <int K, class J>
-cudaError_t run_wave(const J& jobs, WaveState w, uint64_t n_items, uint64_t chunk_items, bool linear,
-                     DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
-  DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
-  DevCounters* const c_shadow = timer->on ? d_cnt + 2 : d_cnt;
-  size_t const smem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
-  static uint32_t g_trace = 0, g_shade = 0, g_shadow = 0, g_gen = 0, g_ptrace = 0, g_pshadow = 0,
-                  g_fb = 0, g_fin = 0;
-  if (!g_trace) {
+const WaveGrids& wave_grids() {
+  static WaveGrids g{};
+  if (!g.trace) {
+    size_t const smem = kTraceSmem;
     cudaFuncSetAttribute(wf_trace<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(wf_shadow<K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(wf_trace_persistent<false, K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(smem));
     cudaFuncSetAttribute(wf_trace_persistent<true, K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(smem));
-    g_trace = persistent_blocks(wf_trace<J>, 128, smem);
-    g_shadow = persistent_blocks(wf_shadow<K, J>, 128, smem);
-    g_ptrace = persistent_blocks(wf_trace_persistent<false, K, J>, 128, smem);
-    g_pshadow = persistent_blocks(wf_trace_persistent<true, K, J>, 128, smem);
-    g_shade = persistent_blocks(wf_shade<K, J>, 128, 0);
-    g_gen = persistent_blocks(wf_generate_stream<K, J>, 256, 0);
-    g_fin = persistent_blocks(wf_finish<K, J>, 256, 0);
-    g_fb = persistent_blocks(wf_trace_fallback<J>, 128, 0);
+    g.shadow = persistent_blocks(wf_shadow<K, J>, 128, smem);
+    g.ptrace = persistent_blocks(wf_trace_persistent<false, K, J>, 128, smem);
+    g.pshadow = persistent_blocks(wf_trace_persistent<true, K, J>, 128, smem);
+    g.shade = persistent_blocks(wf_shade<K, J>, 128, 0);
+    g.gen = persistent_blocks(wf_generate_stream<K, J>, 256, 0);
+    g.fin = persistent_blocks(wf_finish<K, J>, 256, 0);
+    g.fb = persistent_blocks(wf_trace_fallback<J>, 128, 0);
+    g.trace = persistent_blocks(wf_trace<J>, 128, smem);
   }
-  cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
-  // Streaming: every iteration finishes the paths that ended in the last
-  // one, appends new paths behind the queue up to its capacity (plan +
-  // generate), then advances every queued path by one segment (trace,
-  // shade, shadow).
-  for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
-    uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
-    w.c0 = c0;
-    wf_stream_init<<<1, 32, 0, st>>>(w);
-    timer->total++;
-    for (uint32_t it = 0;; it++) {
-      wf_finish<K, J><<<g_fin, 256, 0, st>>>(jobs, w, d_cnt);
-      wf_plan<<<1, 1, 0, st>>>(w, total);
-      wf_generate_stream<K, J><<<g_gen, 256, 0, st>>>(jobs, w, d_cnt);
-      timer->begin(0, st);
-      if (linear) {
-        wf_trace<J><<<g_trace, 128, smem, st>>>(jobs, w, c_closest);
-      } else {
-        wf_trace_persistent<false, K, J><<<g_ptrace, 128, smem, st>>>(jobs, w, c_closest);
-        wf_trace_fallback<J><<<g_fb, 128, 0, st>>>(jobs, w, c_closest);
-      }
-      timer->end(0, st);
-      timer->begin(2, st);
-      wf_shade<K, J><<<g_shade, 128, 0, st>>>(jobs, w, d_cnt);
-      timer->end(2, st);
-      timer->begin(1, st);
-      if (linear) wf_shadow<K, J><<<g_shadow, 128, smem, st>>>(jobs, w, c_shadow);
-      else wf_trace_persistent<true, K, J><<<g_pshadow, 128, smem, st>>>(jobs, w, c_shadow);
-      timer->end(1, st);
-      // finish, plan, generate, trace (+ fallback), shade, shadow
-      timer->total += linear ? 6 : 7;
-      PathBuf const pb = w.in;
-      w.in = w.out;
-      w.out = pb;
-      uint32_t* const pc = w.n_in;
-      w.n_in = w.n_out;
-      w.n_out = pc;
-      // look at the counters every few iterations: done when every work
-      // item was started and the queue is empty
-      if ((it & 3) == 3) {
-        cudaMemcpyAsync(w.h_ctl, w.ctl, kCtlWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) break;
-        timer->harvest();
-        uint32_t const n_in = w.h_ctl[w.n_in - w.ctl];
-        if (w.h_ctl[kCtlNext] == total && n_in == 0) break;
-      }
+  return g;
+}
+
+// Closest hits of the queue `w.in` (the instance BVH kernels, or the
+// reference's linear object loop).
+template <int K, class J>
+void launch_closest(const J& jobs, const WaveState& w, bool linear, DevCounters* cnt, cudaStream_t st) {
+  const WaveGrids& g = wave_grids<K, J>();
+  if (linear) {
+    wf_trace<J><<<g.trace, 128, kTraceSmem, st>>>(jobs, w, cnt);
+  } else {
+    wf_trace_persistent<false, K, J><<<g.ptrace, 128, kTraceSmem, st>>>(jobs, w, cnt);
+    wf_trace_fallback<J><<<g.fb, 128, 0, st>>>(jobs, w, cnt);
+  }
+}
+
+// Swaps the current and next queue after an iteration.
+inline void swap_queues(WaveState& w) {
+  PathBuf const pb = w.in;
+  w.in = w.out;
+  w.out = pb;
+  uint32_t* const pc = w.n_in;
+  w.n_in = w.n_out;
+  w.n_out = pc;
+}
+
+// Every few iterations the host reads the counters: the chunk is done when
+// every work item was started and the queue is empty.
+inline cudaError_t chunk_done(const WaveState& w, uint32_t total, cudaStream_t st, bool& done) {
+  cudaMemcpyAsync(w.h_ctl, w.ctl, kCtlWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+  cudaError_t const e = cudaStreamSynchronize(st);
+  done = e == cudaSuccess && w.h_ctl[kCtlNext] == total && w.h_ctl[w.n_in - w.ctl] == 0;
+  return e;
+}
+
+// One chunk of the streaming wavefront: work items [c0, c0 + total).
+// Every iteration finishes the paths that ended in the last one, appends
+// new paths behind the queue up to its capacity (plan + generate), then
+// advances every queued path by one segment (trace, shade, shadow); the
+// chunk's (sample, pixel) results are then added to the film.
+template <int K, class J>
+cudaError_t wave_chunk(const J& jobs, WaveState& w, uint64_t c0, uint32_t total, bool linear,
+                       DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+  DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
+  DevCounters* const c_shadow = timer->on ? d_cnt + 2 : d_cnt;
+  const WaveGrids& g = wave_grids<K, J>();
+  cudaError_t e = cudaSuccess;
+  w.c0 = c0;
+  wf_stream_init<<<1, 32, 0, st>>>(w);
+  timer->total++;
+  for (uint32_t it = 0;; it++) {
+    wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, w, d_cnt);
+    wf_plan<<<1, 1, 0, st>>>(w, total);
+    wf_generate_stream<K, J><<<g.gen, 256, 0, st>>>(jobs, w, d_cnt);
+    timer->begin(0, st);
+    launch_closest<K>(jobs, w, linear, c_closest, st);
+    timer->end(0, st);
+    timer->begin(2, st);
+    wf_shade<K, J><<<g.shade, 128, 0, st>>>(jobs, w, d_cnt);
+    timer->end(2, st);
+    timer->begin(1, st);
+    if (linear) wf_shadow<K, J><<<g.shadow, 128, kTraceSmem, st>>>(jobs, w, c_shadow);
+    else wf_trace_persistent<true, K, J><<<g.pshadow, 128, kTraceSmem, st>>>(jobs, w, c_shadow);
+    timer->end(1, st);
+    // finish, plan, generate, trace (+ fallback), shade, shadow
+    timer->total += linear ? 6 : 7;
+    swap_queues(w);
+    if ((it & 3) == 3) {
+      bool done = false;
+      e = chunk_done(w, total, st, done);
+      if (e != cudaSuccess) return e;
+      timer->harvest();
+      if (done) break;
     }
-    if (e != cudaSuccess) break;
-    wf_finish<K, J><<<g_fin, 256, 0, st>>>(jobs, w, d_cnt);
-    wf_reduce<J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w, c0 + total);
-    timer->total += 2;
-    e = cudaGetLastError();
   }
-  if (e == cudaSuccess) {
-    wf_finalize<K, J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w);
-    timer->total++;
-    e = cudaGetLastError();
-  }
+  wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, w, d_cnt);
+  wf_reduce<J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w, c0 + total);
+  timer->total += 2;
+  return cudaGetLastError();
+}
+
+template <int K, class J>
+cudaError_t finalize_film(const J& jobs, const WaveState& w, cudaStream_t st, KernelTimer* timer) {
+  wf_finalize<K, J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w);
+  timer->total++;
+  cudaError_t e = cudaGetLastError();
   if (timer->on && e == cudaSuccess) {
     e = cudaStreamSynchronize(st);
     timer->harvest();
   }
+  return e;
+}
+
+// The streaming wavefront over n_items work items of `jobs`, in chunks of
+// at most chunk_items (the capacity of the (sample, pixel) film buffer).
+template <int K, class J>
+cudaError_t run_wave(const J& jobs, WaveState w, uint64_t n_items, uint64_t chunk_items, bool linear,
+                     DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+  cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
+  for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
+    uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
+    e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, timer);
+  }
+  if (e == cudaSuccess) e = finalize_film<K>(jobs, w, st, timer);
   return e;
 }
 

@@ -165,6 +165,7 @@ __global__ void __launch_bounds__(256) wf_generate_stream(J jobs, WaveState w, D
     in.depth[p] = 0;
     in.item[p] = q;
     if (J::kMulti) in.job[p] = jb;
+    if (w.vis) w.vis[q] = 0;
 #pragma unroll
     for (int kk = 0; kk < K; kk++) {
       in.beta[kk * cap + p] = 1.f;
@@ -199,6 +200,10 @@ __global__ void __launch_bounds__(256) wf_finish(J jobs, WaveState w, DevCounter
     }
     nonfinite += finite ? 0u : 1u;
     size_t const o = 3 * size_t(w.e_item[e]);
+    if (w.ltot) {
+#pragma unroll
+      for (int k = 0; k < K; k++) w.ltot[size_t(w.e_item[e]) * K + k] = w.e_acc[k * cap + e];
+    }
     w.sbuf[o] = sx;
     w.sbuf[o + 1] = sy;
     w.sbuf[o + 2] = sz;
@@ -293,6 +298,7 @@ __device__ __forceinline__ void add_shadow(const WaveState& w, uint32_t s) {
   uint32_t const cap = w.cap;
 #pragma unroll
   for (int k = 0; k < K; k++) acc[k * cap + idx] += w.s_contrib[k * cap + s];
+  if (w.vis) w.vis[w.s_item[s]] |= 1ull << w.s_depth[s];
 }
 
 // Persistent instance-BVH traversal of the extension rays (ANY = false,
@@ -434,7 +440,7 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(J jobs, WaveState w, De
 // power heuristic (87-113, its visibility left to the shadow kernel),
 // material importance sample with Russian roulette (115-143).
 template <int K, class J>
-__global__ void __launch_bounds__(128) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
   PathBuf const& in = w.in;
@@ -571,6 +577,10 @@ __global__ void __launch_bounds__(128) wf_shade(J jobs, WaveState w, DevCounters
     if (shadow) {
       w.s_target[s_pos] = cont ? o_pos : (e_pos | kEndedBit);
       if (J::kMulti) w.s_job[s_pos] = jb;
+      if (w.vis) {
+        w.s_item[s_pos] = in.item[i];
+        w.s_depth[s_pos] = in.depth[i];
+      }
       w.sray[0 * cap + s_pos] = sp.x;
       w.sray[1 * cap + s_pos] = sp.y;
       w.sray[2 * cap + s_pos] = sp.z;

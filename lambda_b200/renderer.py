@@ -98,7 +98,9 @@ class Context:
         returns one (height, width, 3) image per job."""
         imgs = []
         for j in jobs:
-            w, h = self.slot_size(j["scene"])
+            s = int(j["scene"])
+            # an unknown slot gets a placeholder; the library rejects the job
+            w, h = self.slot_size(s) if 0 <= s < len(self.flats) else (1, 1)
             imgs.append(np.empty((h, w, 3), np.float32))
         arr = self._jobs(jobs, [im.ctypes.data for im in imgs])
         L.check(self.h, self._lib.lgpu_render_batch(self.h, arr, len(jobs)), "render_batch")
@@ -131,6 +133,36 @@ class Context:
                            seed=seed, spp_offset=spp_offset)
         L.check(self.h, self._lib.lgpu_render_device(self.h, ctypes.byref(p), ctypes.c_void_p(d_out_ptr),
                                                      ctypes.c_void_p(stream or 0)), "render_device")
+
+    def adjoint(self, spp, max_scatterings, sample_p, dloss_dimage, seed=0, flags=0, spp_offset=0,
+                image=False):
+        """Path-replay gradients of a loss whose image gradient is
+        dloss_dimage ((height, width, 3), the render layout).  Returns
+        (grad_spectra (n_spectra, n_bins), grad_materials (n_materials, 4):
+        [thickness, alpha, 0, 0]) and, with image=True, the primal image of
+        the same paths."""
+        w, h = self.size
+        sc = self.flat.scene
+        d = np.ascontiguousarray(dloss_dimage, np.float32).reshape(h, w, 3)
+        gs = np.zeros((int(sc.n_spectra), int(sc.spec.n_bins)), np.float32)
+        gm = np.zeros((int(sc.n_materials), 4), np.float32)
+        img = np.empty((h, w, 3), np.float32) if image else None
+        p = L.RenderParams(spp=spp, max_scatterings=max_scatterings, sample_p=sample_p, flags=flags,
+                           seed=seed, spp_offset=spp_offset)
+        L.check(self.h, self._lib.lgpu_adjoint(self.h, ctypes.byref(p), d.ctypes.data, gs.ctypes.data,
+                                               gm.ctypes.data, img.ctypes.data if image else None),
+                "adjoint")
+        return (gs, gm, img) if image else (gs, gm)
+
+    def adjoint_device(self, spp, max_scatterings, sample_p, d_dimg, d_gspec, d_gmat, d_img=0, seed=0,
+                       flags=0, spp_offset=0, stream=None):
+        """adjoint() on device buffers (pointers)."""
+        p = L.RenderParams(spp=spp, max_scatterings=max_scatterings, sample_p=sample_p, flags=flags,
+                           seed=seed, spp_offset=spp_offset)
+        L.check(self.h, self._lib.lgpu_adjoint_device(self.h, ctypes.byref(p), ctypes.c_void_p(d_dimg),
+                                                      ctypes.c_void_p(d_gspec), ctypes.c_void_p(d_gmat),
+                                                      ctypes.c_void_p(d_img or 0),
+                                                      ctypes.c_void_p(stream or 0)), "adjoint_device")
 
     def trace(self, rays, flags=0):
         rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)

@@ -570,6 +570,22 @@ def blinn_init(m, cfg):
     m.p_spec = F32(F32(m.w_r + m.w_t) / tot)
 
 
+# parsed meshes shared by every scene loaded in this process, keyed by the
+# file's identity (a mesh is read-only once built)
+_MESH_CACHE = {}
+
+
+def _load_mesh(src, path):
+    st = os.stat(path)
+    key = (src, os.path.abspath(path), st.st_mtime_ns, st.st_size)
+    m = _MESH_CACHE.get(key)
+    if m is None:
+        V, N, F = read_obj(path)
+        m = TriMeshData(src, V, N, F)
+        _MESH_CACHE[key] = m
+    return m
+
+
 def load_nls(path, cfg=None, base_dir=None):
     """loadNLS (cg.hpp:2455-2470).  Relative file names inside the scene are
     resolved against base_dir (default: the directory the reference binary is
@@ -627,9 +643,8 @@ def load_nls(path, cfg=None, base_dir=None):
                 src = jo["source"]
                 if src not in mesh_index:
                     p = src if os.path.isabs(src) else os.path.join(base_dir, src)
-                    V, N, F = read_obj(p)
                     mesh_index[src] = len(sc.meshes)
-                    sc.meshes.append(TriMeshData(src, V, N, F))
+                    sc.meshes.append(_load_mesh(src, p))
                 sc.objects.append(Object("trimesh", jo["name"], T, mat, len(sc.objects),
                                          mesh_index[src]))
             else:

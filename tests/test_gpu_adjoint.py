@@ -1,0 +1,120 @@
+"""Path-replay adjoint (lgpu_adjoint) against central finite differences.
+
+The loss is linear in the image, Loss = <w, I> with a fixed seeded weight
+image w, so dLoss/dI = w.  Lambertian albedo bins, thin-film thickness and
+the thin-film IOR do not change any sampling decision, so a device render
+with the same seed at π ± h gives the same paths (common random numbers) and
+the central difference matches the adjoint of those very paths up to the
+difference's truncation and float rounding: the tolerance is 2% relative.
+The lobe exponent α moves sampled directions, so its finite difference and
+the adjoint (which holds sampling fixed) agree only in expectation; they are
+compared at high spp with a statistical tolerance."""
+import numpy as np
+import pytest
+
+from lambda_b200.renderer import Context
+from lambda_b200.scene import FlatScene, load_nls
+
+pytestmark = pytest.mark.gpu
+
+SPP, B, P, SEED = 64, 8, 0.8, 17
+REL_TOL = 0.02
+
+
+@pytest.fixture(scope="module")
+def setup(mixed_nls):
+    sc = load_nls(mixed_nls)
+    flat = FlatScene(sc)
+    ctx = Context()
+    ctx.upload(flat)
+    w_, h_ = ctx.size
+    wimg = np.random.default_rng(5).standard_normal((h_, w_, 3)).astype(np.float32)
+    return ctx, flat, wimg
+
+
+def loss(ctx, flat, wimg, spp=SPP, seed=SEED):
+    ctx.upload(flat)
+    img = ctx.render(spp, B, P, seed=seed)
+    return float(np.sum(img.astype(np.float64) * wimg))
+
+
+def central_fd(ctx, flat, wimg, set_value, x0, h, spp=SPP, seed=SEED):
+    set_value(x0 + h)
+    lp = loss(ctx, flat, wimg, spp, seed)
+    set_value(x0 - h)
+    lm = loss(ctx, flat, wimg, spp, seed)
+    set_value(x0)
+    ctx.upload(flat)
+    return (lp - lm) / (2 * h)
+
+
+def mats_of(flat, kind):
+    return [i for i, m in enumerate(flat.sc.materials) if m.kind == kind]
+
+
+def test_adjoint_primal_image_is_the_render(setup):
+    ctx, flat, wimg = setup
+    gs, gm, img = ctx.adjoint(SPP, B, P, wimg, seed=SEED, image=True)
+    ref = ctx.render(SPP, B, P, seed=SEED)
+    assert np.array_equal(img, ref)
+    assert np.all(np.isfinite(gs)) and np.all(np.isfinite(gm))
+
+
+def test_adjoint_matches_fd_albedo_bins(setup):
+    ctx, flat, wimg = setup
+    gs, gm = ctx.adjoint(SPP, B, P, wimg, seed=SEED)
+    checked = 0
+    for mi in mats_of(flat, "lambertian"):
+        s = flat.materials[mi].spectrum[0]
+        # the bins with the largest gradients of this albedo
+        for b in np.argsort(-np.abs(gs[s]))[:4]:
+            def set_bin(v, s=s, b=b):
+                flat.spectra[s, b] = v
+            x0 = float(flat.spectra[s, b])
+            fd = central_fd(ctx, flat, wimg, set_bin, x0, 1e-3 * max(abs(x0), 0.1))
+            assert abs(gs[s, b] - fd) <= REL_TOL * abs(fd) + 1e-6 * np.abs(gs).max(), (mi, b, gs[s, b], fd)
+            checked += 1
+    assert checked >= 8
+
+
+def test_adjoint_matches_fd_thin_film(setup):
+    ctx, flat, wimg = setup
+    gs, gm = ctx.adjoint(SPP, B, P, wimg, seed=SEED)
+    for mi in mats_of(flat, "thinfilm"):
+        m = flat.materials[mi]
+
+        def set_d(v, m=m):
+            m.d = v
+        fd = central_fd(ctx, flat, wimg, set_d, float(m.d), 0.5)
+        assert abs(gm[mi, 0] - fd) <= REL_TOL * abs(fd), ("thickness", gm[mi, 0], fd)
+        # film IOR: every bin of its spectrum shifted together
+        s = m.spectrum[0]
+        base = flat.spectra[s].copy()
+
+        def set_ior(v, s=s, base=base):
+            flat.spectra[s] = base + np.float32(v)
+        fd = central_fd(ctx, flat, wimg, set_ior, 0.0, 1e-3)
+        g = float(np.sum(gs[s], dtype=np.float64))
+        assert abs(g - fd) <= REL_TOL * abs(fd), ("film ior", g, fd)
+
+
+def test_adjoint_alpha_in_expectation(setup):
+    """α: the adjoint holds sampling fixed, the finite difference lets the
+    sampled directions move with α, so they agree in expectation only.
+    Each is averaged over independent seeds; their difference must be within
+    4 standard errors."""
+    ctx, flat, wimg = setup
+    spp, n_seeds = 512, 8
+    for mi in mats_of(flat, "thinfilm") + mats_of(flat, "blinn")[:1]:
+        m = flat.materials[mi]
+        a0 = float(m.alpha)
+
+        def set_a(v, m=m):
+            m.alpha = v
+        adj = np.array([ctx.adjoint(spp, B, P, wimg, seed=1000 + k)[1][mi, 1] for k in range(n_seeds)],
+                       np.float64)
+        fd = np.array([central_fd(ctx, flat, wimg, set_a, a0, 0.02 * a0, spp=spp, seed=2000 + k)
+                       for k in range(n_seeds)])
+        se = np.sqrt(adj.var(ddof=1) / n_seeds + fd.var(ddof=1) / n_seeds)
+        print("alpha", mi, a0, adj.mean(), fd.mean(), se)
+        assert abs(adj.mean() - fd.mean()) <= 4 * se + 1e-9, (mi, adj.mean(), fd.mean(), se)
