@@ -255,6 +255,98 @@ def run_batched(ctx_cls, device, n_jobs=64):
             "workload": BATCH_DESC}
 
 
+ADJ_DESC = ("inverse-rendering scene: 64x64 thin-film tiles (one object and material each) under 64 "
+            "Lambertian UV spheres (48K tris), 2 quad lights; 512x512, 32 spp, 4 bounces, p=0.8, "
+            "16 hero wavelengths 400-720 nm (80 bins); parameters 64x32 albedo samples + 64x64 thickness")
+
+
+def run_adjoint(device, n_fd=100, reps=3):
+    """Config 4: forward render vs path-replay adjoint (device time, CUDA
+    events), and the adjoint against central finite differences of the
+    device renderer with common random numbers on n_fd random parameters
+    (loss <w, image> with a fixed seeded weight image w)."""
+    import numpy as np
+    import torch
+
+    from lambda_b200 import synth
+    from lambda_b200.inverse import DiffScene
+    rng = np.random.default_rng(4)
+    alb = rng.uniform(0.1, 0.9, (64, synth.ALBEDO_BINS))
+    th = rng.uniform(200.0, 800.0, (64, 64))
+    sc = DiffScene(alb, th, width=512, spp=32, bounces=4, device=device)
+    sc.set_params(alb, th)
+    ctx = sc.ctx
+    H, W, _ = sc.shape
+    wimg = np.random.default_rng(5).standard_normal((H, W, 3)).astype(np.float32)
+    d_w = torch.from_numpy(wimg).cuda()
+    d_img = torch.empty(H * W * 3, dtype=torch.float32, device="cuda")
+    n_spec = int(sc.flat.scene.n_spectra) * int(sc.flat.scene.spec.n_bins)
+    d_gs = torch.empty(n_spec, dtype=torch.float32, device="cuda")
+    d_gm = torch.empty(4 * int(sc.flat.scene.n_materials), dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    def fwd():
+        ctx.render_device(sc.spp, sc.bounces, sc.p, d_img.data_ptr(), seed=7, stream=stream.cuda_stream)
+
+    def adj():
+        ctx.adjoint_device(sc.spp, sc.bounces, sc.p, d_w.data_ptr(), d_gs.data_ptr(), d_gm.data_ptr(), seed=7,
+                           stream=stream.cuda_stream)
+
+    fwd()
+    adj()
+    t_f = min(timed(fwd) for _ in range(reps))
+    t_a = min(timed(adj) for _ in range(reps))
+    g_alb, g_th = sc.gradients(wimg, seed=7)
+    paths = H * W * sc.spp
+
+    def loss():
+        return float(np.sum(sc.render(seed=7).astype(np.float64) * wimg))
+
+    errs, picks = [], []
+    for k in range(n_fd):
+        if rng.uniform() < 0.5:
+            i, j = int(rng.integers(64)), int(rng.integers(synth.ALBEDO_BINS))
+            h, g = 1e-3, g_alb[i, j]
+            a = alb.copy()
+            a[i, j] += h
+            sc.set_params(a, th)
+            lp = loss()
+            a[i, j] -= 2 * h
+            sc.set_params(a, th)
+            lm = loss()
+            picks.append(("albedo", i, j))
+        else:
+            i, j = int(rng.integers(64)), int(rng.integers(64))
+            h, g = 1e-3 * th[i, j], g_th[i, j]
+            t = th.copy()
+            t[i, j] += h
+            sc.set_params(alb, t)
+            lp = loss()
+            t[i, j] -= 2 * h
+            sc.set_params(alb, t)
+            lm = loss()
+            picks.append(("thickness", i, j))
+        fd = (lp - lm) / (2 * h)
+        errs.append((float(g), float(fd)))
+    sc.set_params(alb, th)
+    g = np.array(errs)
+    scale = np.median(np.abs(g[:, 1])) + 1e-30
+    rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 0.01 * scale)
+    return {"forward_s": t_f, "adjoint_s": t_a, "cost_ratio": t_a / t_f,
+            "forward_mpaths_s": paths / t_f / 1e6, "fd_params": n_fd, "fd_h": "1e-3 (albedo) / 1e-3 x thickness",
+            "fd_rel_err_median": float(np.median(rel)), "fd_rel_err_max": float(rel.max()),
+            "fd_within_2pct": int(np.sum(rel <= 0.02)), "workload": ADJ_DESC}
+
+
 def cpu_reference_sample(nls, w, budget_s, fast=True):
     """Times the reference's own pixel loop (oracle/_ref, -O3 OpenMP build)
     over rows spread across the image; returns (paths/s, cores, sample)."""
@@ -413,6 +505,8 @@ def run_device(args, w):
             "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
     if rank == 0 and world == 1 and not args.no_batch:
         line["batched"] = run_batched(Context, local)
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        line["adjoint"] = run_adjoint(local)
     if rank == 0 and world == 1 and not args.no_baseline:
         from oracle import refharness
         if refharness.available(fast=True):
@@ -438,6 +532,7 @@ def main():
     ap.add_argument("--width", type=int, default=None, help="frame width (profiling)")
     ap.add_argument("--no-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential run")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost and FD check")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="seconds of reference CPU work per sampled step")
     args = ap.parse_args()

@@ -253,6 +253,12 @@ int lgpu_abi_version(void);
    host keeps ownership of every array it passed. */
 int lgpu_upload_scene(lgpu_ctx* ctx, const lgpu_scene* scene);
 
+/* Replaces the materials and the spectrum table of the uploaded scene (slot
+   0) without laying out its geometry again; the counts must match the
+   uploaded scene.  For parameter updates in inverse rendering (no
+   counterpart in the reference). */
+int lgpu_update_materials(lgpu_ctx* ctx, const lgpu_scene* scene);
+
 /* Renderer::render (src/renderer.cpp:14-61): renders the uploaded scene into
    the host buffer out_linrgb (cam.width*cam.height*3 floats, row 0 at the
    top). */

@@ -134,6 +134,7 @@ SIGNATURES = {
     "lgpu_upload_scenes": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.POINTER(Scene)), ctypes.c_uint32]),
     "lgpu_render_batch": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32]),
     "lgpu_render_batch_device": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, _vp]),
+    "lgpu_update_materials": (ctypes.c_int, [_vp, ctypes.POINTER(Scene)]),
     "lgpu_render": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp]),
     "lgpu_render_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp]),
     "lgpu_adjoint": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp, _vp, _vp]),

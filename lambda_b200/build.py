@@ -69,7 +69,8 @@ def build(force=False, verbose=False, extra_flags=()):
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(BUILD_DIR, src + ".o")
-        cmds.append([nvcc()] + common + ["-x", "c++", "-c", os.path.join(CSRC, src), "-o", obj])
+        cmds.append([nvcc()] + common + ["-Xcompiler", "-pthread", "-x", "c++", "-c", os.path.join(CSRC, src),
+                                         "-o", obj])
         objs.append(obj)
     procs = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.STDOUT) for c in cmds]
     logs = []
@@ -84,7 +85,7 @@ def build(force=False, verbose=False, extra_flags=()):
     if verbose:
         print("\n".join(logs))
     tmp = OUT + ".tmp"
-    link = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart"]
+    link = [nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-lcudart", "-lpthread"]
     r = subprocess.run(link, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
     if r.returncode != 0:
         sys.stderr.write(r.stdout.decode(errors="replace"))

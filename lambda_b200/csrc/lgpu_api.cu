@@ -17,11 +17,12 @@ namespace {
 template <class T>
 struct DevArray {
   T* ptr = nullptr;
-  size_t n = 0;
+  size_t n = 0;    // elements in use
+  size_t cap = 0;  // elements allocated
   void release() {
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
-    n = 0;
+    n = cap = 0;
   }
 };
 
@@ -108,12 +109,17 @@ int cuda_fail(lgpu_ctx* ctx, cudaError_t e, const char* what) {
   return fail(ctx, code, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Copies h into d, reusing d's allocation when it is large enough.
 template <class T>
 cudaError_t upload(DevArray<T>& d, const std::vector<T>& h, cudaStream_t st) {
-  d.release();
   size_t const n = h.empty() ? 1 : h.size();
-  cudaError_t e = cudaMalloc(&d.ptr, n * sizeof(T));
-  if (e != cudaSuccess) return e;
+  cudaError_t e = cudaSuccess;
+  if (!d.ptr || d.cap < n) {
+    d.release();
+    e = cudaMalloc(&d.ptr, n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    d.cap = n;
+  }
   d.n = h.size();
   if (!h.empty()) e = cudaMemcpyAsync(d.ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st);
   return e;
@@ -121,10 +127,10 @@ cudaError_t upload(DevArray<T>& d, const std::vector<T>& h, cudaStream_t st) {
 
 template <class T>
 cudaError_t ensure(DevArray<T>& d, size_t n) {
-  if (d.n >= n && d.ptr) return cudaSuccess;
+  if (d.cap >= n && d.ptr) return cudaSuccess;
   d.release();
   cudaError_t const e = cudaMalloc(&d.ptr, (n ? n : 1) * sizeof(T));
-  if (e == cudaSuccess) d.n = n;
+  if (e == cudaSuccess) d.n = d.cap = n;
   return e;
 }
 
@@ -551,8 +557,10 @@ int lgpu_upload_scenes(lgpu_ctx* ctx, const lgpu_scene* const* scenes, uint32_t 
       return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "all scenes of a table need the same hero-wavelength count");
   }
   cudaStreamSynchronize(ctx->stream);
-  ctx->release_scene();
+  // slots keep their device allocations for the next upload
+  for (size_t k = n; k < ctx->slots.size(); k++) ctx->slots[k].release();
   ctx->slots.resize(n);
+  ctx->has_scene = false;
   ctx->stats.max_stack = 0;
   uint64_t total = 0;
   for (uint32_t k = 0; k < n; k++) {
@@ -566,6 +574,29 @@ int lgpu_upload_scenes(lgpu_ctx* ctx, const lgpu_scene* const* scenes, uint32_t 
   ctx->S = ctx->slots[0].S;
   ctx->stats.upload_bytes = total;
   ctx->has_scene = true;
+  return LGPU_OK;
+}
+
+int lgpu_update_materials(lgpu_ctx* ctx, const lgpu_scene* scene) {
+  if (!ctx || !scene) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  SceneSlot& sl = ctx->slots[0];
+  if (scene->n_materials != sl.S.n_materials || size_t(scene->n_spectra) * scene->spec.n_bins != sl.spectra.n ||
+      scene->spec.n_bins != sl.S.n_bins || (scene->n_spectra && !scene->spectra))
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT,
+                "the material and spectrum counts must match the uploaded scene");
+  std::vector<DevMaterial> mats;
+  std::string err;
+  if (int rc = make_materials(*scene, mats, err)) return fail(ctx, rc, err);
+  cudaStream_t const st = ctx->stream;
+  cudaError_t e = cudaSuccess;
+  if (!mats.empty())
+    e = cudaMemcpyAsync(sl.mats.ptr, mats.data(), mats.size() * sizeof(DevMaterial), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && sl.spectra.n)
+    e = cudaMemcpyAsync(sl.spectra.ptr, scene->spectra, sl.spectra.n * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "material update");
   return LGPU_OK;
 }
 

@@ -16,7 +16,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <cstring>
+#include <thread>
 #include <memory>
 #include <queue>
 
@@ -273,9 +275,66 @@ bool relayout(const RefView& R, uint32_t slot_base, std::vector<WideNode>& nodes
   return true;
 }
 
+// Runs fn(begin, end) over [0, n) on up to hardware_concurrency threads
+// (one for small n).
+template <class F>
+void parallel_for(size_t n, F fn) {
+  size_t const grain = 1 << 15;
+  size_t nt = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), (n + grain - 1) / grain);
+  if (nt <= 1) {
+    fn(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> ts;
+  size_t const chunk = (n + nt - 1) / nt;
+  for (size_t t = 0; t < nt; t++) {
+    size_t const b = t * chunk, e = std::min(n, b + chunk);
+    if (b < e) ts.emplace_back([=] { fn(b, e); });
+  }
+  for (auto& t : ts) t.join();
+}
+
 bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
 
 }  // namespace
+
+// The material table of a scene (validated), as the kernels read it.
+int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::string& err) {
+  mats.clear();
+  auto spec_ok = [&](int32_t s) { return s >= 0 && uint32_t(s) < sc.n_spectra; };
+  for (uint32_t i = 0; i < sc.n_materials; i++) {
+    const lgpu_material& m = sc.materials[i];
+    DevMaterial d{};
+    d.type = m.type;
+    for (int k = 0; k < 5; k++) d.spectrum[k] = m.spectrum[k];
+    d.alpha = m.alpha;
+    d.p_d = m.p_d;
+    d.p_spec = m.p_spec;
+    d.w_r = m.w_r;
+    d.w_t = m.w_t;
+    d.d = m.d;
+    d.specular = m.specular;
+    int need = 0;
+    switch (m.type) {
+      case LGPU_MAT_LAMBERTIAN: need = 1; break;
+      case LGPU_MAT_BLINN: need = 5; break;
+      case LGPU_MAT_THINFILM: need = 2; break;
+      case LGPU_MAT_MICROFACET: need = 0; break;
+      case LGPU_MAT_EMITTER:
+      case LGPU_MAT_DIREMITTER: need = 1; break;
+      default:
+        err = "unknown material type";
+        return LGPU_ERR_INVALID_ARGUMENT;
+    }
+    for (int k = 0; k < need; k++)
+      if (!spec_ok(m.spectrum[k])) {
+        err = "material spectrum index out of range";
+        return LGPU_ERR_INVALID_ARGUMENT;
+      }
+    mats.push_back(d);
+  }
+  return LGPU_OK;
+}
 
 int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
   L = HostLayout{};
@@ -314,38 +373,7 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
   std::memcpy(L.cmf.data() + 2 * nb, sp.cmf_z, nb * sizeof(float));
 
   auto spec_ok = [&](int32_t s) { return s >= 0 && uint32_t(s) < sc.n_spectra; };
-  // materials
-  for (uint32_t i = 0; i < sc.n_materials; i++) {
-    const lgpu_material& m = sc.materials[i];
-    DevMaterial d{};
-    d.type = m.type;
-    for (int k = 0; k < 5; k++) d.spectrum[k] = m.spectrum[k];
-    d.alpha = m.alpha;
-    d.p_d = m.p_d;
-    d.p_spec = m.p_spec;
-    d.w_r = m.w_r;
-    d.w_t = m.w_t;
-    d.d = m.d;
-    d.specular = m.specular;
-    int need = 0;
-    switch (m.type) {
-      case LGPU_MAT_LAMBERTIAN: need = 1; break;
-      case LGPU_MAT_BLINN: need = 5; break;
-      case LGPU_MAT_THINFILM: need = 2; break;
-      case LGPU_MAT_MICROFACET: need = 0; break;
-      case LGPU_MAT_EMITTER:
-      case LGPU_MAT_DIREMITTER: need = 1; break;
-      default:
-        err = "unknown material type";
-        return LGPU_ERR_INVALID_ARGUMENT;
-    }
-    for (int k = 0; k < need; k++)
-      if (!spec_ok(m.spectrum[k])) {
-        err = "material spectrum index out of range";
-        return LGPU_ERR_INVALID_ARGUMENT;
-      }
-    L.mats.push_back(d);
-  }
+  if (int rc = make_materials(sc, L.mats, err)) return rc;
   // lights
   for (uint32_t i = 0; i < sc.n_lights; i++) {
     const lgpu_light& l = sc.lights[i];
@@ -367,19 +395,26 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       err = "incomplete mesh " + std::to_string(mi);
       return LGPU_ERR_INVALID_ARGUMENT;
     }
-    for (uint32_t f = 0; f < m.n_faces; f++) {
-      const uint32_t* t = m.F + size_t(f) * m.f_stride;
-      for (int k = 0; k < 3; k++)
-        if (t[k] >= m.n_positions || t[3 + k] >= m.n_normals) {
-          err = "face index out of range in mesh " + std::to_string(mi);
-          return LGPU_ERR_INVALID_ARGUMENT;
-        }
-    }
-    for (uint32_t s = 0; s < m.n_prim_idxs; s++)
-      if (m.prim_idxs[s] >= m.n_faces) {
-        err = "BVH primitive index out of range in mesh " + std::to_string(mi);
-        return LGPU_ERR_INVALID_ARGUMENT;
+    std::atomic<bool> bad_face{false}, bad_prim{false};
+    parallel_for(m.n_faces, [&](size_t f0, size_t f1) {
+      for (size_t f = f0; f < f1; f++) {
+        const uint32_t* t = m.F + f * m.f_stride;
+        for (int k = 0; k < 3; k++)
+          if (t[k] >= m.n_positions || t[3 + k] >= m.n_normals) bad_face = true;
       }
+    });
+    parallel_for(m.n_prim_idxs, [&](size_t s0, size_t s1) {
+      for (size_t s = s0; s < s1; s++)
+        if (m.prim_idxs[s] >= m.n_faces) bad_prim = true;
+    });
+    if (bad_face) {
+      err = "face index out of range in mesh " + std::to_string(mi);
+      return LGPU_ERR_INVALID_ARGUMENT;
+    }
+    if (bad_prim) {
+      err = "BVH primitive index out of range in mesh " + std::to_string(mi);
+      return LGPU_ERR_INVALID_ARGUMENT;
+    }
     DevMesh dm{};
     dm.slot_base = uint32_t(L.tris.size());
     dm.face_base = uint32_t(L.shade.size());
@@ -397,34 +432,41 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       return LGPU_ERR_UNSUPPORTED;
     }
     L.max_stack = std::max(L.max_stack, dm.max_stack);
-    for (uint32_t s = 0; s < m.n_prim_idxs; s++) {
-      uint32_t const f = m.prim_idxs[s];
-      const uint32_t* t = m.F + size_t(f) * m.f_stride;
-      TriSlot ts;
-      const float* a = m.V + 3 * size_t(t[0]);
-      const float* b = m.V + 3 * size_t(t[1]);
-      const float* c = m.V + 3 * size_t(t[2]);
-      for (int i = 0; i < 3; i++) {
-        ts.v0[i] = a[i];
-        ts.v1[i] = b[i];
-        ts.v2[i] = c[i];
+    size_t const tri0 = L.tris.size(), shade0 = L.shade.size();
+    L.tris.resize(tri0 + m.n_prim_idxs);
+    L.shade.resize(shade0 + m.n_faces);
+    TriSlot* const tris = L.tris.data() + tri0;
+    FaceShade* const shades = L.shade.data() + shade0;
+    parallel_for(m.n_prim_idxs, [&](size_t s0, size_t s1) {
+      for (size_t s = s0; s < s1; s++) {
+        uint32_t const f = m.prim_idxs[s];
+        const uint32_t* t = m.F + size_t(f) * m.f_stride;
+        TriSlot& ts = tris[s];
+        const float* a = m.V + 3 * size_t(t[0]);
+        const float* b = m.V + 3 * size_t(t[1]);
+        const float* c = m.V + 3 * size_t(t[2]);
+        for (int i = 0; i < 3; i++) {
+          ts.v0[i] = a[i];
+          ts.v1[i] = b[i];
+          ts.v2[i] = c[i];
+        }
+        std::memcpy(&ts.v0[3], &f, 4);
+        ts.v1[3] = 0.f;
+        ts.v2[3] = 0.f;
       }
-      std::memcpy(&ts.v0[3], &f, 4);
-      ts.v1[3] = 0.f;
-      ts.v2[3] = 0.f;
-      L.tris.push_back(ts);
-    }
-    for (uint32_t f = 0; f < m.n_faces; f++) {
-      const uint32_t* t = m.F + size_t(f) * m.f_stride;
-      FaceShade fs;
-      for (int i = 0; i < 3; i++) {
-        fs.n0[i] = m.N[3 * size_t(t[3]) + i];
-        fs.n1[i] = m.N[3 * size_t(t[4]) + i];
-        fs.n2[i] = m.N[3 * size_t(t[5]) + i];
-        fs.gn[i] = m.GN[3 * size_t(f) + i];
+    });
+    parallel_for(m.n_faces, [&](size_t f0, size_t f1) {
+      for (size_t f = f0; f < f1; f++) {
+        const uint32_t* t = m.F + f * m.f_stride;
+        FaceShade& fs = shades[f];
+        for (int i = 0; i < 3; i++) {
+          fs.n0[i] = m.N[3 * size_t(t[3]) + i];
+          fs.n1[i] = m.N[3 * size_t(t[4]) + i];
+          fs.n2[i] = m.N[3 * size_t(t[5]) + i];
+          fs.gn[i] = m.GN[3 * f + i];
+        }
       }
-      L.shade.push_back(fs);
-    }
+    });
     L.meshes.push_back(dm);
   }
   // objects and their world boxes

@@ -52,4 +52,7 @@ struct HostLayout {
 // an lgpu_status with a message in err.
 int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err);
 
+// The validated material table alone (for lgpu_update_materials).
+int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::string& err);
+
 }  // namespace lgpu

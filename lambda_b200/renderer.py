@@ -65,6 +65,11 @@ class Context:
         self._scene_id = id(scene)
         return flat
 
+    def update_materials(self, flat):
+        """Re-sends the materials and spectra of `flat` (same counts as the
+        uploaded scene), e.g. after changing parameters in place."""
+        L.check(self.h, self._lib.lgpu_update_materials(self.h, flat.ptr()), "update_materials")
+
     def upload_many(self, scenes):
         """Scene table for batched renders: scene k goes to slot k (slot 0
         is also the scene of render/trace)."""

@@ -463,3 +463,112 @@ def batch_jobs(n_jobs=64, seed=2024):
                          spp=int(round(np.exp(rng.uniform(np.log(4), np.log(256))))),
                          max_scatterings=int(rng.integers(4, 33)), sample_p=0.8, seed=1000 + k))
     return jobs
+
+
+def uv_sphere(n_lon=24, n_lat=14):
+    """Unit UV sphere: n_lon * (n_lat - 2) * 2 + 2 * n_lon triangles with
+    outward vertex normals; returns V, N, F (0-based)."""
+    V = [(0.0, 0.0, 1.0)]
+    for i in range(1, n_lat):
+        th = np.pi * i / n_lat
+        for j in range(n_lon):
+            ph = 2 * np.pi * j / n_lon
+            V.append((np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)))
+    V.append((0.0, 0.0, -1.0))
+    V = np.asarray(V, np.float64)
+    F = []
+    for j in range(n_lon):
+        F.append((0, 1 + j, 1 + (j + 1) % n_lon))
+    for i in range(n_lat - 2):
+        r0, r1 = 1 + i * n_lon, 1 + (i + 1) * n_lon
+        for j in range(n_lon):
+            a, b = r0 + j, r0 + (j + 1) % n_lon
+            c, d = r1 + j, r1 + (j + 1) % n_lon
+            F.append((a, c, d))
+            F.append((a, d, b))
+    last = len(V) - 1
+    r0 = 1 + (n_lat - 2) * n_lon
+    for j in range(n_lon):
+        F.append((r0 + j, last, r0 + (j + 1) % n_lon))
+    return V, V.copy(), np.asarray(F, np.int64)
+
+
+ALBEDO_BINS = 32
+
+
+def albedo_wavelengths(n=ALBEDO_BINS):
+    """The sample wavelengths of an n-sample albedo on 400-720 nm, as
+    written to (and read back from) its CSV."""
+    return [float("%.6f" % x) for x in np.linspace(400.0, 720.0, n)]
+
+
+def albedo_csv(path, values):
+    """n-sample albedo spectrum on 400-720 nm (the reference's spectral
+    range), read by the reference's box-average loader (cg.hpp:252-272)."""
+    lam = albedo_wavelengths(len(values))
+    with open(path, "w") as f:
+        for l, v in zip(lam, values):
+            f.write("%.6f,%.6f\n" % (l, v))
+
+
+def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.6, alpha=32, seed=9):
+    """The inverse-rendering scene: a ground of G x G thin-film tiles (one
+    2-triangle quad object and material per tile, thickness[i, j] nm) under
+    64 Lambertian UV spheres (624 triangles each, albedo[k] = 32 samples on
+    400-720 nm), lit by two quad lights; about 50K triangles in all.
+    Returns the .nls path."""
+    os.makedirs(out_dir, exist_ok=True)
+    d = os.path.abspath(out_dir)
+    albedo = np.asarray(albedo, np.float64)
+    thickness = np.asarray(thickness, np.float64)
+    G = thickness.shape[0]
+    rng = np.random.default_rng(seed)
+    tile = os.path.join(d, "tile.obj")
+    _write_flat_mesh(tile, [[(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)]])
+    sph = os.path.join(d, "sphere.obj")
+    V, N, F = uv_sphere()
+    write_indexed_obj(sph, V, N, F)
+    blackbody_csv(os.path.join(d, "bb6500.csv"), 6500.0, 4.0)
+    blackbody_csv(os.path.join(d, "bb3500.csv"), 3500.0, 2.5)
+    extent = 8.0
+    s = extent / G
+    materials, objects = [], []
+    for i in range(G):
+        for j in range(G):
+            name = f"film_{i}_{j}"
+            materials.append({"name": name, "type": "thinfilm", "glossiness": alpha,
+                              "thickness": float(thickness[i, j]), "film_ior": {"val": film_ior},
+                              "base_ior": {"val": base_ior}})
+            objects.append({"name": f"tile_{i}_{j}", "type": "trimesh", "material": name, "source": tile,
+                            "transform": {"scale": [s, s, 1],
+                                          "translate": [-extent / 2 + j * s, -extent / 2 + i * s, 0.0]}})
+    n_sph = albedo.shape[0]
+    side = int(np.ceil(np.sqrt(n_sph)))
+    for k in range(n_sph):
+        p = os.path.join(d, f"albedo_{k}.csv")
+        albedo_csv(p, albedo[k])
+        name = f"alb_{k}"
+        materials.append({"name": name, "type": "lambertian", "albedo": {"val": p}})
+        r = 0.22 + 0.08 * float(rng.uniform())
+        gx, gy = k % side, k // side
+        objects.append({"name": f"sphere_{k}", "type": "trimesh", "material": name, "source": sph,
+                        "transform": {"scale": [r, r, r],
+                                      "translate": [(gx - (side - 1) / 2) * extent / side,
+                                                    (gy - (side - 1) / 2) * extent / side, r + 0.05]}})
+    lights = [
+        {"name": "key", "type": "quaddir", "specular": 2,
+         "transform": {"scale": [2.0, 2.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [-3.0, -2.0, 7.0]},
+         "radiance": {"val": os.path.join(d, "bb6500.csv")}},
+        {"name": "fill", "type": "quaddir", "specular": 2,
+         "transform": {"scale": [1.5, 1.5, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [3.0, 3.0, 6.0]},
+         "radiance": {"val": os.path.join(d, "bb3500.csv")}},
+    ]
+    scene = {"camera": {"pos": [0.0, -7.5, 8.5], "look_at": [0.0, -0.3, 0.0], "up": [0, 0, 1],
+                        "fov": 45, "ar": 1.0, "width": width},
+             "materials": materials, "objects": objects, "lights": lights}
+    path = os.path.join(d, "scene.nls")
+    with open(path, "w") as f:
+        json.dump(scene, f)
+    return path

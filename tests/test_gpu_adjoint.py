@@ -105,7 +105,10 @@ def test_adjoint_alpha_in_expectation(setup):
     4 standard errors."""
     ctx, flat, wimg = setup
     spp, n_seeds = 512, 8
-    for mi in mats_of(flat, "thinfilm") + mats_of(flat, "blinn")[:1]:
+    # (Blinn lobes are left out: the reference's pow(h.n, α) of a
+    # back-facing half vector is NaN for the non-even α of a finite
+    # difference, cg.hpp:1810, 1822)
+    for mi in mats_of(flat, "thinfilm"):
         m = flat.materials[mi]
         a0 = float(m.alpha)
 
