@@ -249,10 +249,20 @@ def run_batched(ctx_cls, device, n_jobs=64):
     t_b = timed(batched)
     t_s = timed(sequential)
     equal = all(torch.equal(a, b) for a, b in zip(outs, seq))
-    return {"value": paths / t_b / 1e6, "unit": UNIT, "sequential_value": paths / t_s / 1e6,
-            "speedup": t_s / t_b, "batched_s": t_b, "sequential_s": t_s, "paths": paths,
-            "jobs": n_jobs, "images_identical": bool(equal), "gpu_launches": int(launches),
-            "workload": BATCH_DESC}
+    # the library's autotuner on the same jobs at spp / 16, then the batch
+    # again with the launch shape it chose
+    t0 = time.perf_counter()
+    cfg = ctx.autotune_batch(jobs, spp_divisor=16)
+    tune_s = time.perf_counter() - t0
+    batched()
+    t_t = timed(batched)
+    equal_t = all(torch.equal(a, b) for a, b in zip(outs, seq)) if not cfg["mega_items"] else None
+    return {"value": paths / t_t / 1e6, "unit": UNIT, "sequential_value": paths / t_s / 1e6,
+            "speedup": t_s / t_t, "batched_default_value": paths / t_b / 1e6,
+            "speedup_default_config": t_s / t_b, "batched_s": t_t, "batched_default_s": t_b,
+            "sequential_s": t_s, "paths": paths, "jobs": n_jobs, "images_identical": bool(equal),
+            "images_identical_tuned": equal_t, "autotune": {"config": cfg, "seconds": tune_s},
+            "gpu_launches": int(launches), "workload": BATCH_DESC}
 
 
 ADJ_DESC = ("inverse-rendering scene: 64x64 thin-film tiles (one object and material each) under 64 "
@@ -312,9 +322,13 @@ def run_adjoint(device, n_fd=100, reps=3):
         return float(np.sum(sc.render(seed=7).astype(np.float64) * wimg))
 
     errs, picks = [], []
+    # parameters the image depends on (non-zero adjoint gradient), drawn at
+    # random, half albedo samples and half tile thicknesses
+    live_a = np.argwhere(g_alb != 0)
+    live_t = np.argwhere(g_th != 0)
     for k in range(n_fd):
-        if rng.uniform() < 0.5:
-            i, j = int(rng.integers(64)), int(rng.integers(synth.ALBEDO_BINS))
+        if rng.uniform() < 0.5 or len(live_t) == 0:
+            i, j = (int(x) for x in live_a[rng.integers(len(live_a))])
             h, g = 1e-3, g_alb[i, j]
             a = alb.copy()
             a[i, j] += h
@@ -325,7 +339,7 @@ def run_adjoint(device, n_fd=100, reps=3):
             lm = loss()
             picks.append(("albedo", i, j))
         else:
-            i, j = int(rng.integers(64)), int(rng.integers(64))
+            i, j = (int(x) for x in live_t[rng.integers(len(live_t))])
             h, g = 1e-3 * th[i, j], g_th[i, j]
             t = th.copy()
             t[i, j] += h
@@ -339,12 +353,18 @@ def run_adjoint(device, n_fd=100, reps=3):
         errs.append((float(g), float(fd)))
     sc.set_params(alb, th)
     g = np.array(errs)
-    scale = np.median(np.abs(g[:, 1])) + 1e-30
-    rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 0.01 * scale)
+    rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 1e-30)
+    worst = np.argsort(-rel)[:5]
     return {"forward_s": t_f, "adjoint_s": t_a, "cost_ratio": t_a / t_f,
-            "forward_mpaths_s": paths / t_f / 1e6, "fd_params": n_fd, "fd_h": "1e-3 (albedo) / 1e-3 x thickness",
+            "forward_mpaths_s": paths / t_f / 1e6, "fd_params": n_fd,
+            "fd_params_drawn_from": "parameters with a non-zero adjoint gradient (%d albedo samples, %d "
+                                    "tiles)" % (len(live_a), len(live_t)),
+            "fd_h": "1e-3 (albedo) / 1e-3 x thickness", "fd": "central differences of the device renderer, "
+            "same seed (common random numbers)",
             "fd_rel_err_median": float(np.median(rel)), "fd_rel_err_max": float(rel.max()),
-            "fd_within_2pct": int(np.sum(rel <= 0.02)), "workload": ADJ_DESC}
+            "fd_within_2pct": int(np.sum(rel <= 0.02)),
+            "fd_worst": [[picks[w][0], picks[w][1], picks[w][2], float(g[w, 0]), float(g[w, 1])] for w in worst],
+            "workload": ADJ_DESC}
 
 
 def cpu_reference_sample(nls, w, budget_s, fast=True):

@@ -320,6 +320,29 @@ int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const f
                         float* d_grad_spectra, float* d_grad_materials, float* d_out_linrgb,
                         void* stream);
 
+/* Launch shape of the wavefront renderer (no counterpart in the reference,
+   which renders on CPU threads).  Defaults: queue_cap 2^21, shade_block
+   128, trace_per_sm 0, graphs 1, mega_items 0. */
+typedef struct lgpu_wave_config {
+  uint32_t queue_cap;    /* paths in flight */
+  uint32_t shade_block;  /* threads per block of the shading kernel: 32, 64, 96 or 128 */
+  uint32_t trace_per_sm; /* resident blocks per SM of the persistent trace kernels (0: occupancy limit) */
+  uint32_t graphs;       /* 1: the bounce stages are captured once per chunk as a CUDA graph and replayed */
+  uint64_t mega_items;   /* batched renders: jobs with fewer work items (pixels x spp) are rendered by
+                            the one-thread-per-pixel kernel on a second stream, beside the wavefront */
+} lgpu_wave_config;
+int lgpu_get_wave_config(const lgpu_ctx* ctx, lgpu_wave_config* out);
+int lgpu_set_wave_config(lgpu_ctx* ctx, const lgpu_wave_config* cfg);
+
+/* Autotuner: renders the jobs with spp divided by spp_divisor (at least 1)
+   under candidate launch shapes (queue depth, shading block size, trace
+   occupancy, graphs on/off, megakernel split), one dimension at a time,
+   keeps the fastest (device time) and makes it the context's configuration;
+   writes it to *out when out is not NULL.  Outputs of the jobs are not
+   written. */
+int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_t spp_divisor,
+                        lgpu_wave_config* out);
+
 /* intersect::scene (cg.hpp:1469-1489) on n rays given as 6 floats each
    (origin xyz, direction xyz) in host memory; writes n lgpu_hit. */
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,

@@ -102,6 +102,12 @@ class Job(ctypes.Structure):
                 ("params", RenderParams), ("out", ctypes.c_void_p)]
 
 
+class WaveConfig(ctypes.Structure):
+    _fields_ = [("queue_cap", ctypes.c_uint32), ("shade_block", ctypes.c_uint32),
+                ("trace_per_sm", ctypes.c_uint32), ("graphs", ctypes.c_uint32),
+                ("mega_items", ctypes.c_uint64)]
+
+
 class Hit(ctypes.Structure):
     _fields_ = [("t", ctypes.c_float), ("obj", ctypes.c_uint32), ("face", ctypes.c_uint32),
                 ("mat", ctypes.c_uint32), ("p", ctypes.c_float * 3), ("n", ctypes.c_float * 3),
@@ -139,6 +145,10 @@ SIGNATURES = {
     "lgpu_render_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp]),
     "lgpu_adjoint": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp, _vp, _vp]),
     "lgpu_adjoint_device": (ctypes.c_int, [_vp, ctypes.POINTER(RenderParams), _vp, _vp, _vp, _vp, _vp]),
+    "lgpu_get_wave_config": (ctypes.c_int, [_vp, ctypes.POINTER(WaveConfig)]),
+    "lgpu_set_wave_config": (ctypes.c_int, [_vp, ctypes.POINTER(WaveConfig)]),
+    "lgpu_autotune_batch": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(WaveConfig)]),
     "lgpu_trace_closest": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),
     "lgpu_tonemap": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                     _vp, _vp]),

@@ -356,37 +356,30 @@ __global__ void __launch_bounds__(128) wf_shade_adjoint(OneJob jobs, WaveState w
 // The replay pass over work items [c0, c0 + total).
 template <int K>
 cudaError_t replay_chunk(const OneJob& jobs, WaveState& w, uint64_t c0, uint32_t total, bool linear,
-                         const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
-  static uint32_t g_gen = 0, g_shade = 0;
-  if (!g_gen) {
-    g_gen = persistent_blocks(wf_replay_generate<K>, 256, 0);
-    g_shade = persistent_blocks(wf_shade_adjoint<K>, 128, 0);
+                         const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
+  static uint32_t gen_per_sm = 0, shade_per_sm = 0;
+  if (!gen_per_sm) {
+    gen_per_sm = blocks_per_sm(wf_replay_generate<K>, 256, 0);
+    shade_per_sm = blocks_per_sm(wf_shade_adjoint<K>, 128, 0);
   }
-  DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
+  WaveGrids const gr = wave_grids<K, OneJob>(run->cfg);
+  uint32_t const sms = wave_occupancy<K, OneJob>().sms;
+  DevCounters* const c_closest = run->on ? d_cnt + 1 : d_cnt;
   w.c0 = c0;
   wf_stream_init<<<1, 32, 0, st>>>(w);
-  timer->total++;
-  for (uint32_t it = 0;; it++) {
-    wf_plan<<<1, 1, 0, st>>>(w, total);
-    wf_replay_generate<K><<<g_gen, 256, 0, st>>>(jobs, w, g);
-    timer->begin(0, st);
-    launch_closest<K>(jobs, w, linear, c_closest, st);
-    timer->end(0, st);
-    timer->begin(2, st);
-    wf_shade_adjoint<K><<<g_shade, 128, 0, st>>>(jobs, w, g);
-    timer->end(2, st);
+  run->total++;
+  return run_iterations(w, total, st, run, [&](const WaveState& wi) {
+    wf_plan<<<1, 1, 0, st>>>(wi, total);
+    wf_replay_generate<K><<<sms * gen_per_sm, 256, 0, st>>>(jobs, wi, g);
+    run->begin(0, st);
+    launch_closest<K>(jobs, wi, gr, linear, c_closest, st);
+    run->end(0, st);
+    run->begin(2, st);
+    wf_shade_adjoint<K><<<sms * shade_per_sm, 128, 0, st>>>(jobs, wi, g);
+    run->end(2, st);
     // plan, generate, trace (+ fallback), shade
-    timer->total += linear ? 4 : 5;
-    swap_queues(w);
-    if ((it & 3) == 3) {
-      bool done = false;
-      cudaError_t const e = chunk_done(w, total, st, done);
-      if (e != cudaSuccess) return e;
-      timer->harvest();
-      if (done) break;
-    }
-  }
-  return cudaGetLastError();
+    run->total += linear ? 4 : 5;
+  });
 }
 
 // Primal render (image into d_img when not null) and gradients, chunk by
@@ -394,7 +387,7 @@ cudaError_t replay_chunk(const OneJob& jobs, WaveState& w, uint64_t c0, uint32_t
 template <int K>
 cudaError_t launch_adjoint_k(const DevScene& S, const RenderArgs& a, WaveState* wave, uint64_t chunk_items,
                              float* d_img, const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st,
-                             KernelTimer* timer) {
+                             WaveLaunch* run) {
   OneJob const jobs{S, a, wave->npix, d_img};
   WaveState w = *wave;
   bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
@@ -402,10 +395,10 @@ cudaError_t launch_adjoint_k(const DevScene& S, const RenderArgs& a, WaveState* 
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
   for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
     uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
-    e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, timer);
-    if (e == cudaSuccess) e = replay_chunk<K>(jobs, w, c0, total, linear, g, d_cnt, st, timer);
+    e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, run);
+    if (e == cudaSuccess) e = replay_chunk<K>(jobs, w, c0, total, linear, g, d_cnt, st, run);
   }
-  if (e == cudaSuccess && d_img) e = finalize_film<K>(jobs, w, st, timer);
+  if (e == cudaSuccess && d_img) e = finalize_film<K>(jobs, w, st, run);
   return e;
 }
 

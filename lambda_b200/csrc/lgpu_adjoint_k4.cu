@@ -3,5 +3,5 @@
 
 namespace lgpu {
 template cudaError_t launch_adjoint_k<4>(const DevScene&, const RenderArgs&, WaveState*, uint64_t, float*,
-                                         const AdjointArgs&, DevCounters*, cudaStream_t, KernelTimer*);
+                                         const AdjointArgs&, DevCounters*, cudaStream_t, WaveLaunch*);
 }  // namespace lgpu

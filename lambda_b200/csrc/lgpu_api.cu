@@ -1,6 +1,7 @@
 // lgpu_api.cu — the extern "C" entry points of include/lambda_gpu.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -86,8 +87,13 @@ struct lgpu_ctx {
   DevArray<uint8_t> tm_24;
   DevCounters* counters = nullptr;  // 3 records: all kernels, closest-hit, shadow
   float* exposure = nullptr;
-  KernelTimer timer;
-  bool timer_ready = false;
+  WaveLaunch launch;
+  bool events_ready = false;
+  WaveConfig cfg;     // launch shape of the wavefront
+  GraphCache graph;   // captured bounce stages
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t side = nullptr;  // batches: the megakernel jobs
+  bool keep_counters = false;   // the counters were reset by the caller of a nested render
 
   void release_scene() {
     for (SceneSlot& sl : slots) sl.release();
@@ -140,6 +146,22 @@ int bind_device(lgpu_ctx* ctx) {
   return LGPU_OK;
 }
 
+// Work for a caller's stream runs on the context's own stream (where the
+// bounce stages can be captured as a graph), ordered after what the caller
+// enqueued before the call, and the caller's stream waits for it.
+cudaError_t fork_from(lgpu_ctx* ctx, cudaStream_t user) {
+  if (user == ctx->stream) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(ctx->ev_fork, user);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->stream, ctx->ev_fork, 0);
+  return e;
+}
+cudaError_t join_to(lgpu_ctx* ctx, cudaStream_t user) {
+  if (user == ctx->stream) return cudaSuccess;
+  cudaError_t e = cudaEventRecord(ctx->ev_join, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(user, ctx->ev_join, 0);
+  return e;
+}
+
 // Reads the device counters after a launch, updates the stats and reports
 // device-side checks.
 int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
@@ -166,10 +188,10 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
   ctx->stats.tri_tests = c.tris;
   ctx->stats.inst_tests = c.insts;
   ctx->stats.nonfinite_paths = c.nonfinite;
-  ctx->stats.launches = uint32_t(ctx->timer.total);
+  ctx->stats.launches = uint32_t(ctx->launch.total);
   for (int k = 0; k < 3; k++) {
-    ctx->stats.kernel_ms[k] = timed ? ctx->timer.ms[k] : 0.0;
-    ctx->stats.kernel_launches[k] = timed ? ctx->timer.launches[k] : 0;
+    ctx->stats.kernel_ms[k] = timed ? ctx->launch.ms[k] : 0.0;
+    ctx->stats.kernel_launches[k] = timed ? ctx->launch.launches[k] : 0;
     // counters: [1] closest-hit, [2] shadow; shading does no traversal
     DevCounters const z{};
     const DevCounters& s = (timed && k < 2) ? r[k + 1] : z;
@@ -244,7 +266,8 @@ constexpr uint64_t kSbufBytes = uint64_t(1) << 31;
 int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint64_t n_items, uint64_t chunk_items, bool batch,
                 WaveState& ws, bool adjoint = false) {
   uint32_t const K = ctx->S.hero_k;
-  uint32_t const cap = uint32_t(n_items < kQueueCap ? n_items : kQueueCap);
+  uint64_t const qcap = ctx->cfg.queue_cap ? ctx->cfg.queue_cap : kQueueCap;
+  uint32_t const cap = uint32_t(n_items < qcap ? n_items : qcap);
   size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, adjoint, ws);
   cudaError_t const e = ensure(ctx->w_arena, bytes);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront buffers");
@@ -260,15 +283,17 @@ int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint64_t n_items, uint64_t chunk_i
 }
 
 // Creates the timing events on first use and resets the launch record.
-int prepare_timer(lgpu_ctx* ctx, bool timing) {
-  if (timing && !ctx->timer_ready) {
-    for (auto& k : ctx->timer.ev)
+int prepare_launch(lgpu_ctx* ctx, bool timing) {
+  if (timing && !ctx->events_ready) {
+    for (auto& k : ctx->launch.ev)
       for (auto& s : k)
         for (cudaEvent_t& ev : s)
           if (!ev && cudaEventCreate(&ev) != cudaSuccess) return fail(ctx, LGPU_ERR_CUDA, "timing events");
-    ctx->timer_ready = true;
+    ctx->events_ready = true;
   }
-  ctx->timer.reset(timing);
+  ctx->launch.reset(timing);
+  ctx->launch.cfg = ctx->cfg;
+  ctx->launch.graph = &ctx->graph;
   return LGPU_OK;
 }
 
@@ -302,10 +327,10 @@ int render_scene(lgpu_ctx* ctx, const DevScene& S, const lgpu_render_params* p, 
     ws.n_samples = ns;
     wave = &ws;
   }
-  if (int r = prepare_timer(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) && wave)) return r;
-  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  if (int r = prepare_launch(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) && wave)) return r;
+  cudaError_t e = ctx->keep_counters ? cudaSuccess : cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  if (e == cudaSuccess) e = launch_render(S, a, wave, d_out, ctx->counters, st, &ctx->timer);
+  if (e == cudaSuccess) e = launch_render(S, a, wave, d_out, ctx->counters, st, &ctx->launch);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render launch");
   return LGPU_OK;
@@ -314,6 +339,52 @@ int render_scene(lgpu_ctx* ctx, const DevScene& S, const lgpu_render_params* p, 
 int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaStream_t st) {
   if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
   return render_scene(ctx, ctx->S, p, d_out, st);
+}
+
+int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_outs, cudaStream_t st);
+
+// A batch split by the megakernel threshold: the small jobs render with the
+// one-thread-per-pixel kernel on the side stream while the others take the
+// wavefront on st.
+int batch_split(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_outs, cudaStream_t st,
+                const std::vector<uint32_t>& wave_jobs, const std::vector<uint32_t>& mega_jobs) {
+  (void)n;
+  if (!ctx->side) {
+    cudaError_t const e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "side stream");
+  }
+  if (int r = prepare_launch(ctx, false)) return r;
+  cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_fork, st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+  for (uint32_t k : mega_jobs) {
+    if (e != cudaSuccess) break;
+    const DevScene& S = ctx->slots[jobs[k].scene].S;
+    lgpu_render_params p = jobs[k].params;
+    p.flags |= LGPU_FLAG_MEGAKERNEL;
+    e = launch_render(S, render_args(&p, S), nullptr, d_outs[k], ctx->counters, ctx->side, &ctx->launch);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_join, ctx->side);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "megakernel jobs");
+  unsigned long long const mega_launches = ctx->launch.total;
+  int rc = LGPU_OK;
+  if (!wave_jobs.empty()) {
+    std::vector<lgpu_job> wj;
+    std::vector<float*> wo;
+    for (uint32_t k : wave_jobs) {
+      wj.push_back(jobs[k]);
+      wo.push_back(d_outs[k]);
+    }
+    // the counters were reset above and the megakernel jobs already count
+    ctx->keep_counters = true;
+    rc = batch_impl(ctx, wj.data(), uint32_t(wj.size()), wo.data(), st);
+    ctx->keep_counters = false;
+  }
+  e = cudaStreamWaitEvent(st, ctx->ev_join, 0);
+  ctx->launch.total += mega_launches;
+  if (rc != LGPU_OK) return rc;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "megakernel join");
+  return LGPU_OK;
 }
 
 // Renders the jobs (outputs d_outs, device) in one streaming wavefront; a
@@ -331,6 +402,14 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
     linear = linear || (jobs[k].params.flags & LGPU_FLAG_REFERENCE_ORDER);
   }
   if (n == 1) return render_scene(ctx, ctx->slots[jobs[0].scene].S, &jobs[0].params, d_outs[0], st);
+  // jobs below the megakernel threshold run on the side stream
+  std::vector<uint32_t> wave_jobs, mega_jobs;
+  for (uint32_t k = 0; k < n; k++) {
+    const lgpu_camera& c = ctx->slots[jobs[k].scene].S.cam;
+    uint64_t const items = uint64_t(c.width) * c.height * jobs[k].params.spp;
+    ((ctx->cfg.mega_items && items < ctx->cfg.mega_items) ? mega_jobs : wave_jobs).push_back(k);
+  }
+  if (!mega_jobs.empty()) return batch_split(ctx, jobs, n, d_outs, st, wave_jobs, mega_jobs);
   std::vector<DevJob> hj(n);
   std::vector<uint64_t> items(n + 1);
   std::vector<uint32_t> pixels(n + 1);
@@ -367,12 +446,12 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch tables");
   WaveState ws{};
   if (int r = ensure_wave(ctx, uint32_t(px), g, chunk, true, ws)) return r;
-  if (int r = prepare_timer(ctx, timing)) return r;
-  e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  if (int r = prepare_launch(ctx, timing)) return r;
+  e = ctx->keep_counters ? cudaSuccess : cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
   if (e == cudaSuccess)
     e = launch_batch(ctx->S.hero_k, ctx->jobs.ptr, ctx->job_items.ptr, ctx->job_pixels.ptr, n, g, chunk, linear,
-                     &ws, ctx->counters, st, &ctx->timer);
+                     &ws, ctx->counters, st, &ctx->launch);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   // the host tables must outlive their asynchronous copies
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -400,14 +479,14 @@ int adjoint_impl(lgpu_ctx* ctx, const lgpu_render_params* p, const float* d_dimg
   uint64_t const chunk = n_items < max_items ? n_items : max_items;
   WaveState ws{};
   if (int r = ensure_wave(ctx, a.pixel_count, n_items, chunk, false, ws, true)) return r;
-  if (int r = prepare_timer(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) != 0)) return r;
+  if (int r = prepare_launch(ctx, (p->flags & LGPU_FLAG_KERNEL_TIMING) != 0)) return r;
   size_t const n_spec = ctx->slots[0].spectra.n;
   cudaError_t e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_gspec, 0, n_spec * sizeof(float), st);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_gmat, 0, 4 * size_t(S.n_materials) * sizeof(float), st);
   AdjointArgs const g{d_dimg, d_gspec, d_gmat};
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  if (e == cudaSuccess) e = launch_adjoint(S.hero_k, S, a, &ws, chunk, d_img, g, ctx->counters, st, &ctx->timer);
+  if (e == cudaSuccess) e = launch_adjoint(S.hero_k, S, a, &ws, chunk, d_img, g, ctx->counters, st, &ctx->launch);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint launch");
   return LGPU_OK;
@@ -499,6 +578,8 @@ int lgpu_create(int device, lgpu_ctx** out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->counters, 3 * sizeof(DevCounters));
   if (e == cudaSuccess) e = cudaMalloc(&ctx->exposure, sizeof(float));
   if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, kCtlWords * sizeof(uint32_t));
@@ -533,10 +614,17 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->exposure) cudaFree(ctx->exposure);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
-  for (auto& k : ctx->timer.ev)
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+  ctx->graph.release();
+  for (auto& k : ctx->launch.ev)
     for (auto& s : k)
       for (cudaEvent_t ev : s)
         if (ev) cudaEventDestroy(ev);
+  if (ctx->side) {
+    cudaStreamSynchronize(ctx->side);
+    cudaStreamDestroy(ctx->side);
+  }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -603,13 +691,13 @@ int lgpu_update_materials(lgpu_ctx* ctx, const lgpu_scene* scene) {
 int lgpu_render_device(lgpu_ctx* ctx, const lgpu_render_params* params, float* d_out, void* stream) {
   if (!ctx || !d_out) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (int r = bind_device(ctx)) return r;
-  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-  int const rc = render_impl(ctx, params, d_out, st);
+  cudaStream_t const user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaError_t e = fork_from(ctx, user);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
+  int const rc = render_impl(ctx, params, d_out, ctx->stream);
   if (rc != LGPU_OK) return rc;
-  if (st != ctx->stream) {
-    cudaError_t const e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
-  }
+  e = join_to(ctx, user);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render");
   return collect(ctx, "render", timing_requested(params));
 }
 
@@ -630,15 +718,15 @@ int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linr
 int lgpu_render_batch_device(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, void* stream) {
   if (!ctx || !jobs || n == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument or no job");
   if (int r = bind_device(ctx)) return r;
-  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaStream_t const user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
   std::vector<float*> outs(n);
   for (uint32_t k = 0; k < n; k++) outs[k] = jobs[k].out;
-  int const rc = batch_impl(ctx, jobs, n, outs.data(), st);
+  cudaError_t e = fork_from(ctx, user);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render batch");
+  int const rc = batch_impl(ctx, jobs, n, outs.data(), ctx->stream);
   if (rc != LGPU_OK) return rc;
-  if (st != ctx->stream) {
-    cudaError_t const e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "render batch");
-  }
+  e = join_to(ctx, user);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "render batch");
   return collect(ctx, "render batch", batch_timing(jobs, n));
 }
 
@@ -672,10 +760,13 @@ int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const f
   if (!ctx || !params || !d_dloss_dimage || !d_grad_spectra || !d_grad_materials)
     return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (int r = bind_device(ctx)) return r;
-  cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-  int const rc = adjoint_impl(ctx, params, d_dloss_dimage, d_grad_spectra, d_grad_materials, d_out_linrgb, st);
+  cudaStream_t const user = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+  cudaError_t e = fork_from(ctx, user);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint");
+  int const rc = adjoint_impl(ctx, params, d_dloss_dimage, d_grad_spectra, d_grad_materials, d_out_linrgb,
+                              ctx->stream);
   if (rc != LGPU_OK) return rc;
-  cudaError_t const e = cudaStreamSynchronize(st);
+  e = join_to(ctx, user);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "adjoint");
   return collect(ctx, "adjoint", (params->flags & LGPU_FLAG_KERNEL_TIMING) != 0);
 }
@@ -709,6 +800,108 @@ int lgpu_adjoint(lgpu_ctx* ctx, const lgpu_render_params* params, const float* d
   return collect(ctx, "adjoint", (params->flags & LGPU_FLAG_KERNEL_TIMING) != 0);
 }
 
+int lgpu_get_wave_config(const lgpu_ctx* ctx, lgpu_wave_config* out) {
+  if (!ctx || !out) return LGPU_ERR_INVALID_ARGUMENT;
+  out->queue_cap = ctx->cfg.queue_cap;
+  out->shade_block = ctx->cfg.shade_block;
+  out->trace_per_sm = ctx->cfg.trace_per_sm;
+  out->graphs = ctx->cfg.graphs;
+  out->mega_items = ctx->cfg.mega_items;
+  return LGPU_OK;
+}
+
+int lgpu_set_wave_config(lgpu_ctx* ctx, const lgpu_wave_config* c) {
+  if (!ctx || !c) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (c->queue_cap < 1024 || c->queue_cap > (1u << 24))
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "queue_cap must be in [1024, 2^24]");
+  if (c->shade_block < 32 || c->shade_block > 128 || c->shade_block % 32)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "shade_block must be 32, 64, 96 or 128");
+  ctx->cfg.queue_cap = c->queue_cap;
+  ctx->cfg.shade_block = c->shade_block;
+  ctx->cfg.trace_per_sm = c->trace_per_sm;
+  ctx->cfg.graphs = c->graphs ? 1 : 0;
+  ctx->cfg.mega_items = c->mega_items;
+  return LGPU_OK;
+}
+
+int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_t spp_divisor,
+                        lgpu_wave_config* out) {
+  if (!ctx || !jobs || n == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument or no job");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  uint32_t const div = spp_divisor ? spp_divisor : 1;
+  std::vector<lgpu_job> sample(jobs, jobs + n);
+  std::vector<size_t> off(n + 1, 0);
+  for (uint32_t k = 0; k < n; k++) {
+    if (sample[k].scene >= ctx->slots.size())
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": no such scene");
+    sample[k].params.spp = std::max(1u, sample[k].params.spp / div);
+    sample[k].params.flags &= ~uint32_t(LGPU_FLAG_KERNEL_TIMING);
+    const lgpu_camera& c = ctx->slots[sample[k].scene].S.cam;
+    off[k + 1] = off[k] + size_t(c.width) * c.height * 3;
+  }
+  cudaError_t e = ensure(ctx->batch_out, off[n]);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "autotune output buffer");
+  std::vector<float*> outs(n);
+  for (uint32_t k = 0; k < n; k++) outs[k] = ctx->batch_out.ptr + off[k];
+  // device time of the sample batch under the current configuration
+  auto measure = [&](double& ms) -> int {
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; rep++) {
+      cudaEvent_t e0 = ctx->ev0, e1 = ctx->ev1;
+      cudaError_t ce = cudaEventRecord(e0, ctx->stream);
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "autotune");
+      int const rc = batch_impl(ctx, sample.data(), n, outs.data(), ctx->stream);
+      if (rc != LGPU_OK) return rc;
+      ce = cudaEventRecord(e1, ctx->stream);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+      float t = 0.f;
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&t, e0, e1);
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "autotune");
+      best = std::min(best, t);
+    }
+    ms = best;
+    return LGPU_OK;
+  };
+  WaveConfig const saved = ctx->cfg;
+  WaveConfig best = ctx->cfg;
+  double best_ms = 0.0;
+  if (int rc = measure(best_ms)) {
+    ctx->cfg = saved;
+    return rc;
+  }
+  // coordinate descent over the knobs, each from the best so far
+  auto try_dim = [&](auto set, std::initializer_list<uint64_t> values) -> int {
+    WaveConfig const base = best;
+    for (uint64_t v : values) {
+      ctx->cfg = base;
+      set(ctx->cfg, v);
+      if (std::memcmp(&ctx->cfg, &base, sizeof(WaveConfig)) == 0) continue;
+      double ms = 0.0;
+      if (int rc = measure(ms)) return rc;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = ctx->cfg;
+      }
+    }
+    return LGPU_OK;
+  };
+  int rc = try_dim([](WaveConfig& c, uint64_t v) { c.queue_cap = uint32_t(v); },
+                   {1u << 19, 1u << 20, 1u << 21, 1u << 22});
+  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.shade_block = uint32_t(v); }, {64, 96, 128});
+  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.trace_per_sm = uint32_t(v); }, {0, 4, 5});
+  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.graphs = uint32_t(v); }, {0, 1});
+  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.mega_items = v; }, {0, 1u << 14, 1u << 16});
+  if (rc) {
+    ctx->cfg = saved;
+    return rc;
+  }
+  ctx->cfg = best;
+  ctx->stats.last_kernel_ms = best_ms;
+  if (out) lgpu_get_wave_config(ctx, out);
+  return LGPU_OK;
+}
+
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {
   if (!ctx || (n && (!rays || !out))) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (int r = bind_device(ctx)) return r;
@@ -721,8 +914,8 @@ int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t fl
   e = cudaMemcpyAsync(ctx->rays.ptr, rays, 6 * n * sizeof(float), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
-  ctx->timer.reset(false);
-  ctx->timer.total = 1;
+  ctx->launch.reset(false);
+  ctx->launch.total = 1;
   if (e == cudaSuccess) e = launch_trace(ctx->S, ctx->rays.ptr, n, flags, ctx->hits.ptr, ctx->counters, st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
   if (e == cudaSuccess)

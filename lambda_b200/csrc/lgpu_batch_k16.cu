@@ -3,5 +3,5 @@
 
 namespace lgpu {
 template cudaError_t launch_batch_k<16>(const DevJob*, const uint64_t*, const uint32_t*, uint32_t, uint64_t,
-                                       uint64_t, bool, WaveState*, DevCounters*, cudaStream_t, KernelTimer*);
+                                       uint64_t, bool, WaveState*, DevCounters*, cudaStream_t, WaveLaunch*);
 }  // namespace lgpu

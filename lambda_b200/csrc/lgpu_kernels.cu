@@ -130,12 +130,12 @@ cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uin
 }
 
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                          DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+                          DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
   if (a.pixel_count == 0) return cudaSuccess;
   switch (S.hero_k) {
-    case 4: return launch_render_k<4>(S, a, wave, d_out, d_cnt, st, timer);
-    case 8: return launch_render_k<8>(S, a, wave, d_out, d_cnt, st, timer);
-    case 16: return launch_render_k<16>(S, a, wave, d_out, d_cnt, st, timer);
+    case 4: return launch_render_k<4>(S, a, wave, d_out, d_cnt, st, run);
+    case 8: return launch_render_k<8>(S, a, wave, d_out, d_cnt, st, run);
+    case 16: return launch_render_k<16>(S, a, wave, d_out, d_cnt, st, run);
   }
   return cudaErrorInvalidValue;
 }
@@ -143,29 +143,29 @@ cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wav
 cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* d_item_bases,
                          const uint32_t* d_pix_bases, uint32_t n_jobs, uint64_t n_items,
                          uint64_t chunk_items, bool linear, WaveState* wave, DevCounters* d_cnt,
-                         cudaStream_t st, KernelTimer* timer) {
+                         cudaStream_t st, WaveLaunch* run) {
   if (n_jobs == 0 || n_items == 0) return cudaSuccess;
   switch (hero_k) {
     case 4:
       return launch_batch_k<4>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
-                               d_cnt, st, timer);
+                               d_cnt, st, run);
     case 8:
       return launch_batch_k<8>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
-                               d_cnt, st, timer);
+                               d_cnt, st, run);
     case 16:
       return launch_batch_k<16>(d_jobs, d_item_bases, d_pix_bases, n_jobs, n_items, chunk_items, linear, wave,
-                                d_cnt, st, timer);
+                                d_cnt, st, run);
   }
   return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_adjoint(uint32_t hero_k, const DevScene& S, const RenderArgs& a, WaveState* wave,
                            uint64_t chunk_items, float* d_img, const AdjointArgs& g, DevCounters* d_cnt,
-                           cudaStream_t st, KernelTimer* timer) {
+                           cudaStream_t st, WaveLaunch* run) {
   switch (hero_k) {
-    case 4: return launch_adjoint_k<4>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
-    case 8: return launch_adjoint_k<8>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
-    case 16: return launch_adjoint_k<16>(S, a, wave, chunk_items, d_img, g, d_cnt, st, timer);
+    case 4: return launch_adjoint_k<4>(S, a, wave, chunk_items, d_img, g, d_cnt, st, run);
+    case 8: return launch_adjoint_k<8>(S, a, wave, chunk_items, d_img, g, d_cnt, st, run);
+    case 16: return launch_adjoint_k<16>(S, a, wave, chunk_items, d_img, g, d_cnt, st, run);
   }
   return cudaErrorInvalidValue;
 }

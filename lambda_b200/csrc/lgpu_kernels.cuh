@@ -93,13 +93,36 @@ struct RenderArgs {
 cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
                          lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st);
 
-// Launch bookkeeping of one render: the number of kernel launches, and
-// with `on` the device time of the wavefront's launches per kind (0
-// closest-hit traversal, 1 shadow traversal, 2 shading), from pairs of
-// events recorded around each launch and read back after the stream
-// synchronises.
-struct KernelTimer {
+// Launch shape of the wavefront, chosen by the autotuner
+// (lgpu_autotune_batch) or set by the caller (lgpu_set_wave_config).
+struct WaveConfig {
+  uint32_t queue_cap = 1u << 21;  // paths in flight
+  uint32_t shade_block = 128;     // threads per block of the shading kernel (32, 64 or 128)
+  uint32_t trace_per_sm = 0;      // persistent trace blocks per SM (0: the occupancy limit)
+  uint32_t graphs = 1;            // 1: bounce stages replayed from a captured CUDA graph
+  uint64_t mega_items = 0;        // batches: jobs with fewer work items run the megakernel
+};
+
+// Instantiated CUDA graph of the bounce stages, updated in place while the
+// stages keep their shape.
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+  }
+};
+
+// Launch settings and bookkeeping of one render: the configuration, the
+// graph cache, the number of kernel launches, and with `on` the device time
+// of the wavefront's launches per kind (0 closest-hit traversal, 1 shadow
+// traversal, 2 shading), from pairs of events recorded around each launch
+// and read back after the stream synchronises (no graphs then).
+struct WaveLaunch {
   static constexpr int kSlots = 16;
+  WaveConfig cfg;
+  GraphCache* graph = nullptr;
+  unsigned long long graph_launches = 0;
   bool on = false;
   unsigned long long total = 0;  // kernel launches
   cudaEvent_t ev[3][kSlots][2] = {};
@@ -109,6 +132,7 @@ struct KernelTimer {
   void reset(bool timing) {
     on = timing;
     total = 0;
+    graph_launches = 0;
     for (int k = 0; k < 3; k++) {
       used[k] = 0;
       ms[k] = 0.0;
@@ -208,20 +232,20 @@ struct JobTable {
 cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* d_item_bases,
                          const uint32_t* d_pix_bases, uint32_t n_jobs, uint64_t n_items,
                          uint64_t chunk_items, bool linear, WaveState* wave, DevCounters* d_cnt,
-                         cudaStream_t st, KernelTimer* timer);
+                         cudaStream_t st, WaveLaunch* run);
 template <int K>
 cudaError_t launch_batch_k(const DevJob* d_jobs, const uint64_t* d_item_bases, const uint32_t* d_pix_bases,
                            uint32_t n_jobs, uint64_t n_items, uint64_t chunk_items, bool linear,
-                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run);
 
 // Renders with the wavefront kernels when wave != nullptr, else with the
 // one-thread-per-pixel megakernel.  d_cnt points at 3 counter records:
-// everything, and with timer->on the closest-hit and shadow traversal apart.
+// everything, and with run->on the closest-hit and shadow traversal apart.
 template <int K>
 cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+                            DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run);
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                          DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer);
+                          DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run);
 
 // Path-replay adjoint (lgpu_adjoint.cuh): primal image (d_img, may be null)
 // and gradients of the loss whose image gradient is dimg.
@@ -232,11 +256,11 @@ struct AdjointArgs {
 };
 cudaError_t launch_adjoint(uint32_t hero_k, const DevScene& S, const RenderArgs& a, WaveState* wave,
                            uint64_t chunk_items, float* d_img, const AdjointArgs& g, DevCounters* d_cnt,
-                           cudaStream_t st, KernelTimer* timer);
+                           cudaStream_t st, WaveLaunch* run);
 template <int K>
 cudaError_t launch_adjoint_k(const DevScene& S, const RenderArgs& a, WaveState* wave, uint64_t chunk_items,
                              float* d_img, const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st,
-                             KernelTimer* timer);
+                             WaveLaunch* run);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
 // doubles, at least tonemap_partials_needed(n)).

@@ -84,28 +84,26 @@ __global__ void __launch_bounds__(128) render_kernel(DevScene S, RenderArgs a, f
   flush_counters(cnt, rays, paths, ts, nonfinite);
 }
 
-// Persistent grid size: every SM filled to its occupancy limit.
-template <class F>
-uint32_t persistent_blocks(F kernel, int threads, size_t smem) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-  if (per_sm < 1) per_sm = 1;
-  return uint32_t(sms * per_sm);
-}
-
-// Launch grids of the wavefront kernels: every SM filled to the kernel's
-// occupancy limit (computed once per instantiation).
-struct WaveGrids {
-  uint32_t trace, shade, shadow, gen, ptrace, pshadow, fb, fin;
+// Blocks per SM each wavefront kernel can keep resident (computed once per
+// instantiation; the shading kernel per block size).
+struct WaveOccupancy {
+  uint32_t sms = 0;
+  uint32_t trace, shadow, ptrace, pshadow, gen, fin, fb;
+  uint32_t shade[5];  // 32, 64, 96, 128 threads per block (index block / 32)
 };
 constexpr size_t kTraceSmem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
 
+template <class F>
+uint32_t blocks_per_sm(F kernel, int threads, size_t smem) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  return uint32_t(per_sm < 1 ? 1 : per_sm);
+}
+
 template <int K, class J>
-const WaveGrids& wave_grids() {
-  static WaveGrids g{};
-  if (!g.trace) {
+const WaveOccupancy& wave_occupancy() {
+  static WaveOccupancy o{};
+  if (!o.sms) {
     size_t const smem = kTraceSmem;
     cudaFuncSetAttribute(wf_trace<J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
     cudaFuncSetAttribute(wf_shadow<K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
@@ -113,23 +111,53 @@ const WaveGrids& wave_grids() {
                          int(smem));
     cudaFuncSetAttribute(wf_trace_persistent<true, K, J>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          int(smem));
-    g.shadow = persistent_blocks(wf_shadow<K, J>, 128, smem);
-    g.ptrace = persistent_blocks(wf_trace_persistent<false, K, J>, 128, smem);
-    g.pshadow = persistent_blocks(wf_trace_persistent<true, K, J>, 128, smem);
-    g.shade = persistent_blocks(wf_shade<K, J>, 128, 0);
-    g.gen = persistent_blocks(wf_generate_stream<K, J>, 256, 0);
-    g.fin = persistent_blocks(wf_finish<K, J>, 256, 0);
-    g.fb = persistent_blocks(wf_trace_fallback<J>, 128, 0);
-    g.trace = persistent_blocks(wf_trace<J>, 128, smem);
+    o.trace = blocks_per_sm(wf_trace<J>, 128, smem);
+    o.shadow = blocks_per_sm(wf_shadow<K, J>, 128, smem);
+    o.ptrace = blocks_per_sm(wf_trace_persistent<false, K, J>, 128, smem);
+    o.pshadow = blocks_per_sm(wf_trace_persistent<true, K, J>, 128, smem);
+    o.gen = blocks_per_sm(wf_generate_stream<K, J>, 256, 0);
+    o.fin = blocks_per_sm(wf_finish<K, J>, 256, 0);
+    o.fb = blocks_per_sm(wf_trace_fallback<J>, 128, 0);
+    for (int b = 1; b <= 4; b++) o.shade[b] = blocks_per_sm(wf_shade<K, J>, 32 * b, 0);
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    o.sms = uint32_t(sms);
   }
+  return o;
+}
+
+// Grids of one render: every SM filled to the kernel's occupancy limit, or
+// to the configured cap for the persistent trace kernels.
+struct WaveGrids {
+  uint32_t trace, shade, shade_block, shadow, gen, ptrace, pshadow, fb, fin;
+};
+
+template <int K, class J>
+WaveGrids wave_grids(const WaveConfig& cfg) {
+  const WaveOccupancy& o = wave_occupancy<K, J>();
+  uint32_t const sb = (cfg.shade_block >= 32 && cfg.shade_block <= 128 && cfg.shade_block % 32 == 0)
+                          ? cfg.shade_block
+                          : 128;
+  auto cap = [&](uint32_t per_sm) { return cfg.trace_per_sm && cfg.trace_per_sm < per_sm ? cfg.trace_per_sm : per_sm; };
+  WaveGrids g;
+  g.trace = o.sms * o.trace;
+  g.shade_block = sb;
+  g.shade = o.sms * o.shade[sb / 32];
+  g.shadow = o.sms * o.shadow;
+  g.gen = o.sms * o.gen;
+  g.ptrace = o.sms * cap(o.ptrace);
+  g.pshadow = o.sms * cap(o.pshadow);
+  g.fb = o.sms * o.fb;
+  g.fin = o.sms * o.fin;
   return g;
 }
 
 // Closest hits of the queue `w.in` (the instance BVH kernels, or the
 // reference's linear object loop).
 template <int K, class J>
-void launch_closest(const J& jobs, const WaveState& w, bool linear, DevCounters* cnt, cudaStream_t st) {
-  const WaveGrids& g = wave_grids<K, J>();
+void launch_closest(const J& jobs, const WaveState& w, const WaveGrids& g, bool linear, DevCounters* cnt,
+                    cudaStream_t st) {
   if (linear) {
     wf_trace<J><<<g.trace, 128, kTraceSmem, st>>>(jobs, w, cnt);
   } else {
@@ -148,13 +176,75 @@ inline void swap_queues(WaveState& w) {
   w.n_out = pc;
 }
 
-// Every few iterations the host reads the counters: the chunk is done when
-// every work item was started and the queue is empty.
-inline cudaError_t chunk_done(const WaveState& w, uint32_t total, cudaStream_t st, bool& done) {
-  cudaMemcpyAsync(w.h_ctl, w.ctl, kCtlWords * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-  cudaError_t const e = cudaStreamSynchronize(st);
-  done = e == cudaSuccess && w.h_ctl[kCtlNext] == total && w.h_ctl[w.n_in - w.ctl] == 0;
-  return e;
+// The chunk is done when every work item was started and the queue is
+// empty (the host copy of the counters, after the stream synchronised).
+inline bool chunk_done(const WaveState& w, uint32_t total) {
+  return w.h_ctl[kCtlNext] == total && w.h_ctl[w.n_in - w.ctl] == 0;
+}
+
+constexpr int kItersPerCheck = 4;
+
+// Runs iterations of a chunk (issue(w) enqueues one iteration's kernels)
+// until the chunk is done, reading the counters back every kItersPerCheck
+// iterations.  With a graph cache and no per-kernel timing, the
+// kItersPerCheck iterations and the counter readback are captured once as a
+// CUDA graph and replayed; the graph's kernel arguments alternate the two
+// queues, so the state is back in its starting parity after each replay.
+template <class Issue>
+cudaError_t run_iterations(WaveState& w, uint32_t total, cudaStream_t st, WaveLaunch* run, Issue issue) {
+  size_t const ctl_bytes = kCtlWords * sizeof(uint32_t);
+  bool graph = run->graph && run->cfg.graphs && !run->on;
+  unsigned long long per_graph = 0;  // kernel launches in one replay
+  if (graph) {
+    cudaGraph_t gph = nullptr;
+    unsigned long long const t0 = run->total;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      WaveState wc = w;
+      for (int k = 0; k < kItersPerCheck; k++) {
+        issue(wc);
+        swap_queues(wc);
+      }
+      cudaMemcpyAsync(w.h_ctl, w.ctl, ctl_bytes, cudaMemcpyDeviceToHost, st);
+      e = cudaStreamEndCapture(st, &gph);
+    }
+    per_graph = run->total - t0;
+    run->total = t0;
+    if (e == cudaSuccess) {
+      GraphCache& gc = *run->graph;
+      cudaGraphExecUpdateResultInfo info;
+      if (!gc.exec || cudaGraphExecUpdate(gc.exec, gph, &info) != cudaSuccess) {
+        cudaGetLastError();
+        gc.release();
+        e = cudaGraphInstantiate(&gc.exec, gph, 0);
+      }
+    }
+    if (gph) cudaGraphDestroy(gph);
+    if (e != cudaSuccess) {
+      // capture is not possible on this stream (e.g. the legacy default
+      // stream): launch the kernels one by one
+      cudaGetLastError();
+      graph = false;
+    }
+  }
+  for (;;) {
+    if (graph) {
+      cudaError_t const e = cudaGraphLaunch(run->graph->exec, st);
+      if (e != cudaSuccess) return e;
+      run->graph_launches++;
+      run->total += per_graph;
+    } else {
+      for (int k = 0; k < kItersPerCheck; k++) {
+        issue(w);
+        swap_queues(w);
+      }
+      cudaMemcpyAsync(w.h_ctl, w.ctl, ctl_bytes, cudaMemcpyDeviceToHost, st);
+    }
+    cudaError_t const e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    run->harvest();
+    if (chunk_done(w, total)) return cudaSuccess;
+  }
 }
 
 // One chunk of the streaming wavefront: work items [c0, c0 + total).
@@ -164,53 +254,45 @@ inline cudaError_t chunk_done(const WaveState& w, uint32_t total, cudaStream_t s
 // chunk's (sample, pixel) results are then added to the film.
 template <int K, class J>
 cudaError_t wave_chunk(const J& jobs, WaveState& w, uint64_t c0, uint32_t total, bool linear,
-                       DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
-  DevCounters* const c_closest = timer->on ? d_cnt + 1 : d_cnt;
-  DevCounters* const c_shadow = timer->on ? d_cnt + 2 : d_cnt;
-  const WaveGrids& g = wave_grids<K, J>();
-  cudaError_t e = cudaSuccess;
+                       DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
+  DevCounters* const c_closest = run->on ? d_cnt + 1 : d_cnt;
+  DevCounters* const c_shadow = run->on ? d_cnt + 2 : d_cnt;
+  WaveGrids const g = wave_grids<K, J>(run->cfg);
   w.c0 = c0;
   wf_stream_init<<<1, 32, 0, st>>>(w);
-  timer->total++;
-  for (uint32_t it = 0;; it++) {
-    wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, w, d_cnt);
-    wf_plan<<<1, 1, 0, st>>>(w, total);
-    wf_generate_stream<K, J><<<g.gen, 256, 0, st>>>(jobs, w, d_cnt);
-    timer->begin(0, st);
-    launch_closest<K>(jobs, w, linear, c_closest, st);
-    timer->end(0, st);
-    timer->begin(2, st);
-    wf_shade<K, J><<<g.shade, 128, 0, st>>>(jobs, w, d_cnt);
-    timer->end(2, st);
-    timer->begin(1, st);
-    if (linear) wf_shadow<K, J><<<g.shadow, 128, kTraceSmem, st>>>(jobs, w, c_shadow);
-    else wf_trace_persistent<true, K, J><<<g.pshadow, 128, kTraceSmem, st>>>(jobs, w, c_shadow);
-    timer->end(1, st);
+  run->total++;
+  cudaError_t e = run_iterations(w, total, st, run, [&](const WaveState& wi) {
+    wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, wi, d_cnt);
+    wf_plan<<<1, 1, 0, st>>>(wi, total);
+    wf_generate_stream<K, J><<<g.gen, 256, 0, st>>>(jobs, wi, d_cnt);
+    run->begin(0, st);
+    launch_closest<K>(jobs, wi, g, linear, c_closest, st);
+    run->end(0, st);
+    run->begin(2, st);
+    wf_shade<K, J><<<g.shade, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
+    run->end(2, st);
+    run->begin(1, st);
+    if (linear) wf_shadow<K, J><<<g.shadow, 128, kTraceSmem, st>>>(jobs, wi, c_shadow);
+    else wf_trace_persistent<true, K, J><<<g.pshadow, 128, kTraceSmem, st>>>(jobs, wi, c_shadow);
+    run->end(1, st);
     // finish, plan, generate, trace (+ fallback), shade, shadow
-    timer->total += linear ? 6 : 7;
-    swap_queues(w);
-    if ((it & 3) == 3) {
-      bool done = false;
-      e = chunk_done(w, total, st, done);
-      if (e != cudaSuccess) return e;
-      timer->harvest();
-      if (done) break;
-    }
-  }
+    run->total += linear ? 6 : 7;
+  });
+  if (e != cudaSuccess) return e;
   wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, w, d_cnt);
   wf_reduce<J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w, c0 + total);
-  timer->total += 2;
+  run->total += 2;
   return cudaGetLastError();
 }
 
 template <int K, class J>
-cudaError_t finalize_film(const J& jobs, const WaveState& w, cudaStream_t st, KernelTimer* timer) {
+cudaError_t finalize_film(const J& jobs, const WaveState& w, cudaStream_t st, WaveLaunch* run) {
   wf_finalize<K, J><<<(w.npix + 255) / 256, 256, 0, st>>>(jobs, w);
-  timer->total++;
+  run->total++;
   cudaError_t e = cudaGetLastError();
-  if (timer->on && e == cudaSuccess) {
+  if (run->on && e == cudaSuccess) {
     e = cudaStreamSynchronize(st);
-    timer->harvest();
+    run->harvest();
   }
   return e;
 }
@@ -219,38 +301,38 @@ cudaError_t finalize_film(const J& jobs, const WaveState& w, cudaStream_t st, Ke
 // at most chunk_items (the capacity of the (sample, pixel) film buffer).
 template <int K, class J>
 cudaError_t run_wave(const J& jobs, WaveState w, uint64_t n_items, uint64_t chunk_items, bool linear,
-                     DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+                     DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
   for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
     uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
-    e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, timer);
+    e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, run);
   }
-  if (e == cudaSuccess) e = finalize_film<K>(jobs, w, st, timer);
+  if (e == cudaSuccess) e = finalize_film<K>(jobs, w, st, run);
   return e;
 }
 
 template <int K>
 cudaError_t launch_render_k(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
-                            DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+                            DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
   if (!wave) {
     uint32_t const blocks = (a.pixel_count + 127) / 128;
     render_kernel<K><<<blocks, 128, 0, st>>>(S, a, d_out, d_cnt);
-    timer->total++;
+    run->total++;
     return cudaGetLastError();
   }
   OneJob const jobs{S, a, wave->npix, d_out};
   // the instance BVH kernels, or the reference's linear object loop
   bool const linear = (a.flags & LGPU_FLAG_REFERENCE_ORDER) || S.n_objects <= 4;
   return run_wave<K>(jobs, *wave, uint64_t(wave->npix) * a.spp, uint64_t(wave->npix) * wave->n_samples,
-                     linear, d_cnt, st, timer);
+                     linear, d_cnt, st, run);
 }
 
 template <int K>
 cudaError_t launch_batch_k(const DevJob* d_jobs, const uint64_t* d_item_bases, const uint32_t* d_pix_bases,
                            uint32_t n_jobs, uint64_t n_items, uint64_t chunk_items, bool linear,
-                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, KernelTimer* timer) {
+                           WaveState* wave, DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
   JobTable const jobs{d_jobs, d_item_bases, d_pix_bases, n_jobs};
-  return run_wave<K>(jobs, *wave, n_items, chunk_items, linear, d_cnt, st, timer);
+  return run_wave<K>(jobs, *wave, n_items, chunk_items, linear, d_cnt, st, run);
 }
 
 }  // namespace lgpu

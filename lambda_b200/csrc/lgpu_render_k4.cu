@@ -3,5 +3,5 @@
 
 namespace lgpu {
 template cudaError_t launch_render_k<4>(const DevScene&, const RenderArgs&, WaveState*, float*,
-                                        DevCounters*, cudaStream_t, KernelTimer*);
+                                        DevCounters*, cudaStream_t, WaveLaunch*);
 }  // namespace lgpu

@@ -142,9 +142,9 @@ def run_inverse(iters=20, width=128, spp=8, target_spp=1024, grid=64, n_spheres=
             th.clamp_(100.0, 900.0)
         err_th = float(np.sqrt(np.mean((th.detach().numpy() - th_true) ** 2)))
         err_alb = float(np.sqrt(np.mean((alb.detach().numpy() - alb_true) ** 2)))
-        hist.append((float(loss), err_th, err_alb))
+        hist.append((float(loss.detach()), err_th, err_alb))
         log("iter %3d  loss %.6e  thickness rmse %.1f nm  albedo rmse %.4f  (%.2f s)" %
-            (it, float(loss), err_th, err_alb, time.perf_counter() - t0))
+            (it, hist[-1][0], err_th, err_alb, time.perf_counter() - t0))
     return hist
 
 

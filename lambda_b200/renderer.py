@@ -97,6 +97,28 @@ class Context:
             arr[k].out = o
         return arr
 
+    def wave_config(self):
+        c = L.WaveConfig()
+        L.check(self.h, self._lib.lgpu_get_wave_config(self.h, ctypes.byref(c)), "get_wave_config")
+        return {k: getattr(c, k) for k, _ in L.WaveConfig._fields_}
+
+    def set_wave_config(self, **kw):
+        """Changes fields of the wavefront launch shape (queue_cap,
+        shade_block, trace_per_sm, graphs, mega_items)."""
+        cur = self.wave_config()
+        cur.update(kw)
+        c = L.WaveConfig(**cur)
+        L.check(self.h, self._lib.lgpu_set_wave_config(self.h, ctypes.byref(c)), "set_wave_config")
+
+    def autotune_batch(self, jobs, spp_divisor=16):
+        """Runs the library's autotuner on the jobs (spp / spp_divisor) and
+        returns the launch shape it chose (now the context's)."""
+        arr = self._jobs(jobs, [0] * len(jobs))
+        c = L.WaveConfig()
+        L.check(self.h, self._lib.lgpu_autotune_batch(self.h, arr, len(jobs), spp_divisor, ctypes.byref(c)),
+                "autotune_batch")
+        return {k: getattr(c, k) for k, _ in L.WaveConfig._fields_}
+
     def render_batch(self, jobs):
         """Renders every job (dicts: scene, spp, max_scatterings, sample_p
         and optionally seed, flags, spp_offset) in one batched launch;

@@ -511,7 +511,7 @@ def albedo_csv(path, values):
             f.write("%.6f,%.6f\n" % (l, v))
 
 
-def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.6, alpha=32, seed=9):
+def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.6, alpha=8, seed=9):
     """The inverse-rendering scene: a ground of G x G thin-film tiles (one
     2-triangle quad object and material per tile, thickness[i, j] nm) under
     64 Lambertian UV spheres (624 triangles each, albedo[k] = 32 samples on
@@ -555,14 +555,16 @@ def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.
                         "transform": {"scale": [r, r, r],
                                       "translate": [(gx - (side - 1) / 2) * extent / side,
                                                     (gy - (side - 1) / 2) * extent / side, r + 0.05]}})
+    # the lights' mirror images in the ground fall inside the view, so the
+    # thin-film highlights (whose colour the thickness sets) are seen
     lights = [
         {"name": "key", "type": "quaddir", "specular": 2,
-         "transform": {"scale": [2.0, 2.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
-                       "translate": [-3.0, -2.0, 7.0]},
+         "transform": {"scale": [3.0, 3.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [0.0, 3.0, 7.0]},
          "radiance": {"val": os.path.join(d, "bb6500.csv")}},
         {"name": "fill", "type": "quaddir", "specular": 2,
-         "transform": {"scale": [1.5, 1.5, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
-                       "translate": [3.0, 3.0, 6.0]},
+         "transform": {"scale": [2.0, 2.0, 1], "rotate": {"axis": [1, 0, 0], "degrees": 180},
+                       "translate": [2.5, 5.0, 6.0]},
          "radiance": {"val": os.path.join(d, "bb3500.csv")}},
     ]
     scene = {"camera": {"pos": [0.0, -7.5, 8.5], "look_at": [0.0, -0.3, 0.0], "up": [0, 0, 1],

@@ -88,3 +88,42 @@ def test_batch_rejects_bad_jobs(scenes):
     with pytest.raises(L.LgpuError):
         ctx.render_batch([dict(scene=0, spp=0, max_scatterings=1, sample_p=0.8),
                           dict(scene=1, spp=1, max_scatterings=1, sample_p=0.8)])
+
+
+def test_image_independent_of_launch_shape(scenes):
+    """Queue depth, shading block size, trace occupancy and graph replay
+    change only the schedule: images are bit-identical."""
+    ctx = Context()
+    ctx.upload_many(scenes)
+    ref = ctx.render_batch(JOBS[:4])
+    plain = Context()
+    plain.upload(scenes[1])
+    p_ref = plain.render(JOBS[1]["spp"], JOBS[1]["max_scatterings"], JOBS[1]["sample_p"], seed=JOBS[1]["seed"])
+    for shape in (dict(queue_cap=4096), dict(shade_block=64), dict(trace_per_sm=3), dict(graphs=0),
+                  dict(queue_cap=1 << 22, shade_block=96, graphs=1)):
+        ctx.set_wave_config(**shape)
+        got = ctx.render_batch(JOBS[:4])
+        for a, b in zip(got, ref):
+            assert np.array_equal(a, b), shape
+        plain.set_wave_config(**shape)
+        p = plain.render(JOBS[1]["spp"], JOBS[1]["max_scatterings"], JOBS[1]["sample_p"], seed=JOBS[1]["seed"])
+        assert np.array_equal(p, p_ref), shape
+
+
+def test_megakernel_split_and_autotune(scenes):
+    ctx = Context()
+    ctx.upload_many(scenes)
+    ref = ctx.render_batch(JOBS)
+    # the smallest jobs on the megakernel: same estimator and random
+    # streams, different arithmetic order, so statistically equal images
+    ctx.set_wave_config(mega_items=48 * 48 * 4)
+    got = ctx.render_batch(JOBS)
+    for a, b in zip(got, ref):
+        assert a.shape == b.shape and np.all(np.isfinite(a))
+        assert abs(float(a.mean()) - float(b.mean())) <= 0.05 * abs(float(b.mean())) + 1e-6
+    cfg = ctx.autotune_batch(JOBS, spp_divisor=2)
+    assert cfg == ctx.wave_config()
+    ctx.set_wave_config(mega_items=0)
+    again = ctx.render_batch(JOBS)
+    for a, b in zip(again, ref):
+        assert np.array_equal(a, b)
