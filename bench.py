@@ -321,50 +321,53 @@ def run_adjoint(device, n_fd=100, reps=3):
     def loss():
         return float(np.sum(sc.render(seed=7).astype(np.float64) * wimg))
 
-    errs, picks = [], []
-    # parameters the image depends on (non-zero adjoint gradient), drawn at
-    # random, half albedo samples and half tile thicknesses
-    live_a = np.argwhere(g_alb != 0)
-    live_t = np.argwhere(g_th != 0)
-    for k in range(n_fd):
-        if rng.uniform() < 0.5 or len(live_t) == 0:
-            i, j = (int(x) for x in live_a[rng.integers(len(live_a))])
-            h, g = 1e-3, g_alb[i, j]
-            a = alb.copy()
-            a[i, j] += h
-            sc.set_params(a, th)
-            lp = loss()
-            a[i, j] -= 2 * h
-            sc.set_params(a, th)
-            lm = loss()
-            picks.append(("albedo", i, j))
-        else:
-            i, j = (int(x) for x in live_t[rng.integers(len(live_t))])
-            h, g = 1e-3 * th[i, j], g_th[i, j]
-            t = th.copy()
-            t[i, j] += h
-            sc.set_params(alb, t)
-            lp = loss()
-            t[i, j] -= 2 * h
-            sc.set_params(alb, t)
-            lm = loss()
-            picks.append(("thickness", i, j))
-        fd = (lp - lm) / (2 * h)
-        errs.append((float(g), float(fd)))
-    sc.set_params(alb, th)
-    g = np.array(errs)
-    rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 1e-30)
-    worst = np.argsort(-rel)[:5]
+    def fd_check(h_alb, h_th_rel):
+        """central differences with the given steps on n_fd random parameters"""
+        frng = np.random.default_rng(11)
+        live_a = np.argwhere(g_alb != 0)
+        live_t = np.argwhere(g_th != 0)
+        out = []
+        for k in range(n_fd):
+            if frng.uniform() < 0.5 or len(live_t) == 0:
+                i, j = (int(x) for x in live_a[frng.integers(len(live_a))])
+                h, g = h_alb, g_alb[i, j]
+                a = alb.copy()
+                a[i, j] += h
+                sc.set_params(a, th)
+                lp = loss()
+                a[i, j] -= 2 * h
+                sc.set_params(a, th)
+                lm = loss()
+                name = "albedo"
+            else:
+                i, j = (int(x) for x in live_t[frng.integers(len(live_t))])
+                h, g = h_th_rel * th[i, j], g_th[i, j]
+                t = th.copy()
+                t[i, j] += h
+                sc.set_params(alb, t)
+                lp = loss()
+                t[i, j] -= 2 * h
+                sc.set_params(alb, t)
+                lm = loss()
+                name = "thickness"
+            out.append((name, i, j, float(g), (lp - lm) / (2 * h)))
+        sc.set_params(alb, th)
+        g = np.array([[o[3], o[4]] for o in out])
+        rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 1e-30)
+        worst = np.argsort(-rel)[:3]
+        return {"h": "%g (albedo) / %g x thickness" % (h_alb, h_th_rel),
+                "rel_err_median": float(np.median(rel)), "rel_err_max": float(rel.max()),
+                "within_2pct": int(np.sum(rel <= 0.02)), "worst": [list(out[w]) for w in worst],
+                "drawn_from": "%d albedo samples, %d tiles with a non-zero adjoint gradient" %
+                              (len(live_a), len(live_t))}
+
+    fd3 = fd_check(1e-3, 1e-3)
+    fd2 = fd_check(1e-2, 1e-2)
     return {"forward_s": t_f, "adjoint_s": t_a, "cost_ratio": t_a / t_f,
             "forward_mpaths_s": paths / t_f / 1e6, "fd_params": n_fd,
-            "fd_params_drawn_from": "parameters with a non-zero adjoint gradient (%d albedo samples, %d "
-                                    "tiles)" % (len(live_a), len(live_t)),
-            "fd_h": "1e-3 (albedo) / 1e-3 x thickness", "fd": "central differences of the device renderer, "
-            "same seed (common random numbers)",
-            "fd_rel_err_median": float(np.median(rel)), "fd_rel_err_max": float(rel.max()),
-            "fd_within_2pct": int(np.sum(rel <= 0.02)),
-            "fd_worst": [[picks[w][0], picks[w][1], picks[w][2], float(g[w, 0]), float(g[w, 1])] for w in worst],
-            "workload": ADJ_DESC}
+            "fd": "central differences of the device renderer, same seed (common random numbers), loss "
+                  "<w, image> with a seeded normal weight image; relative error |adjoint - fd| / |fd|",
+            "fd_h1e-3": fd3, "fd_h1e-2": fd2, "workload": ADJ_DESC}
 
 
 def cpu_reference_sample(nls, w, budget_s, fast=True):

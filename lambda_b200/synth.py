@@ -85,7 +85,13 @@ def _quad(p0, p1, p2, p3):
 
 def _write_flat_mesh(path, quads):
     """OBJ of planar quads with one flat normal per quad: normal = (p1-p0) x
-    (p2-p0), the geometric normal the reference loader computes."""
+    (p2-p0), the geometric normal the reference loader computes.
+
+    A mesh's bounds include fast_obj's dummy vertex at the origin
+    (cg.hpp:2215-2229), and the reference never hits a mesh whose bounds
+    are flat (its slab test needs t_min < t_max, cg.hpp:1268-1286): a single
+    quad through the origin's plane is therefore written one unit off that
+    plane and moved back by its object transform."""
     V, N, F = [], [], []
     for q in quads:
         base = len(V)
@@ -128,7 +134,9 @@ def box_room(out_dir, width=256, light_peak=6.0):
     # inward walls: bottom, top, back, left, right (the -y side is open)
     white = [walls[0], walls[1], walls[3]]
     _write_flat_mesh(os.path.join(d, "walls_white.obj"), white)
-    _write_flat_mesh(os.path.join(d, "wall_left.obj"), [walls[4]])
+    # the left wall lies in the plane x = 0 of the dummy vertex: written at
+    # x = 1 and moved back by the object transform
+    _write_flat_mesh(os.path.join(d, "wall_left.obj"), [[(x + 1, y, z) for (x, y, z) in walls[4]]])
     _write_flat_mesh(os.path.join(d, "wall_right.obj"), [walls[5]])
     _write_flat_mesh(os.path.join(d, "block_tall.obj"),
                      _box_quads((0.2, 0.45, 0.0), (0.5, 0.75, 0.6)))
@@ -149,7 +157,7 @@ def box_room(out_dir, width=256, light_peak=6.0):
         "objects": [
             {"name": "walls", "type": "trimesh", "transform": {},
              "material": "white", "source": os.path.join(d, "walls_white.obj")},
-            {"name": "left", "type": "trimesh", "transform": {},
+            {"name": "left", "type": "trimesh", "transform": {"translate": [-1, 0, 0]},
              "material": "left", "source": os.path.join(d, "wall_left.obj")},
             {"name": "right", "type": "trimesh", "transform": {},
              "material": "right", "source": os.path.join(d, "wall_right.obj")},
@@ -339,13 +347,16 @@ def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 
     if not os.path.exists(mesh_path):
         V, N, F = displaced_icosphere(subdiv, seed)
         write_indexed_obj(mesh_path, V, N, F)
+    # written at z = 1, moved to z = 0 by the object transform (flat bounds
+    # through the dummy vertex are never hit, see _write_flat_mesh)
     _write_flat_mesh(os.path.join(d, "ground.obj"),
-                     [[(-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0)]])
+                     [[(-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1)]])
     blackbody_csv(os.path.join(d, "bb6500.csv"), 6500.0, 3.0)
     blackbody_csv(os.path.join(d, "bb4000.csv"), 4000.0, 2.0)
     materials = [{"name": "ground", "type": "lambertian", "albedo": {"val": 0.5}}]
     objects = [{"name": "ground", "type": "trimesh", "material": "ground",
-                "transform": {"scale": [12, 12, 1]}, "source": os.path.join(d, "ground.obj")}]
+                "transform": {"scale": [12, 12, 1], "translate": [0, 0, -1]},
+                "source": os.path.join(d, "ground.obj")}]
     side = int(np.ceil(np.sqrt(n_instances)))
     spacing = 1.1
     for i in range(n_instances):
@@ -524,7 +535,8 @@ def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.
     G = thickness.shape[0]
     rng = np.random.default_rng(seed)
     tile = os.path.join(d, "tile.obj")
-    _write_flat_mesh(tile, [[(0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0)]])
+    # the tile quad at z = 1, moved to z = 0 by each tile's transform
+    _write_flat_mesh(tile, [[(0, 0, 1), (1, 0, 1), (1, 1, 1), (0, 1, 1)]])
     sph = os.path.join(d, "sphere.obj")
     V, N, F = uv_sphere()
     write_indexed_obj(sph, V, N, F)
@@ -541,7 +553,7 @@ def diff_scene(out_dir, albedo, thickness, width=512, film_ior=1.45, base_ior=1.
                               "base_ior": {"val": base_ior}})
             objects.append({"name": f"tile_{i}_{j}", "type": "trimesh", "material": name, "source": tile,
                             "transform": {"scale": [s, s, 1],
-                                          "translate": [-extent / 2 + j * s, -extent / 2 + i * s, 0.0]}})
+                                          "translate": [-extent / 2 + j * s, -extent / 2 + i * s, -1.0]}})
     n_sph = albedo.shape[0]
     side = int(np.ceil(np.sqrt(n_sph)))
     for k in range(n_sph):
