@@ -370,9 +370,44 @@ def run_adjoint(device, n_fd=100, reps=3):
             "fd_h1e-3": fd3, "fd_h1e-2": fd2, "workload": ADJ_DESC}
 
 
-def cpu_reference_sample(nls, w, budget_s, fast=True):
+def rmse_check(ctx, w, ref_rows, d_out, stream, oracle_renders=16):
+    """Relative RMSE per channel, over the reference's sampled rows, of the
+    device image and of the reference's own image at the workload's spp,
+    both against an FP64 mean of oracle_renders device renders of that spp
+    with other random streams (the high-spp oracle image)."""
+    import numpy as np
+    import torch
+    W, H = ctx.size
+    spp, B, p = w["spp"], w["bounces"], w["p"]
+    acc = np.zeros((H, W, 3), np.float64)
+    for k in range(oracle_renders):
+        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=999, spp_offset=k * spp,
+                          stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        acc += d_out.cpu().numpy().reshape(H, W, 3)
+    oracle = acc / oracle_renders
+    ctx.render_device(spp, B, p, d_out.data_ptr(), seed=1, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    gpu = d_out.cpu().numpy().reshape(H, W, 3).astype(np.float64)
+    rows = sorted(ref_rows)
+    # scene row r is image row H - 1 - r
+    o = np.stack([oracle[H - 1 - r] for r in rows])
+    g = np.stack([gpu[H - 1 - r] for r in rows])
+    c = np.stack([ref_rows[r].astype(np.float64) for r in rows])
+    den = np.sqrt(np.mean(o ** 2, axis=(0, 1)))
+    e_g = np.sqrt(np.mean((g - o) ** 2, axis=(0, 1))) / den
+    e_c = np.sqrt(np.mean((c - o) ** 2, axis=(0, 1))) / den
+    return {"device": [float(x) for x in e_g], "reference": [float(x) for x in e_c],
+            "ratio": [float(x) for x in e_g / e_c], "rows": len(rows),
+            "oracle": "device, %d spp (%d renders of %d spp with other random streams, FP64 mean)" %
+                      (oracle_renders * spp, oracle_renders, spp),
+            "what": "relative RMSE per channel (R, G, B) over the reference's sampled rows at %d spp" % spp}
+
+
+def cpu_reference_sample(nls, w, budget_s, fast=True, keep=None):
     """Times the reference's own pixel loop (oracle/_ref, -O3 OpenMP build)
-    over rows spread across the image; returns (paths/s, cores, sample)."""
+    over rows spread across the image; returns (paths/s, cores, sample).
+    With a dict `keep`, the rendered rows are stored in it by scene row."""
     from oracle import refharness
     ref = refharness.RefScene(nls, fast=fast)
     cores = ref.L.ref_max_threads()
@@ -385,7 +420,9 @@ def cpu_reference_sample(nls, w, budget_s, fast=True):
                       [i * (H - 1) / max(n_rows - 1, 1) for i in range(n_rows)]))
     t0 = time.perf_counter()
     for r in rows:
-        ref.render_rows(w["spp"], w["bounces"], w["p"], r, r + 1)
+        img = ref.render_rows(w["spp"], w["bounces"], w["p"], r, r + 1)
+        if keep is not None:
+            keep[r] = img[0]
     dt = time.perf_counter() - t0
     paths = len(rows) * ref.width * w["spp"]
     sample = "%d of %d rows (evenly spread) x %d px x %d spp = %d paths" % (
@@ -533,9 +570,11 @@ def run_device(args, w):
     if rank == 0 and world == 1 and not args.no_baseline:
         from oracle import refharness
         if refharness.available(fast=True):
-            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
+            rows = {}
+            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s, keep=rows)
             line["cpu_baseline"] = {"value": v / 1e6, "unit": UNIT, "cores": cores,
                                     "kind": "reference", "sample": sample}
+            line["rmse"] = rmse_check(ctx, w, rows, d_out, stream)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

@@ -435,6 +435,50 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(J jobs, WaveState w, De
 
 // ---- shade ------------------------------------------------------------------------
 
+// Material sort within a block: the block's queue entries [base, base +
+// blockDim.x) are handed to its threads grouped by what the shading kernel
+// will do with them (miss, then material type, then past the queue end), so
+// a warp's lanes take the same branch of the BSDF code.  A counting sort:
+// per warp one ballot per group, a shared table of the warps' counts, and
+// each thread's rank within its group.  Returns the entry for this thread.
+constexpr int kSortGroups = 8;
+
+template <class J>
+__device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveState& w, uint32_t base, uint32_t n) {
+  __shared__ uint32_t counts[kSortGroups][4];
+  __shared__ uint16_t perm[128];
+  uint32_t const t = threadIdx.x, lane = t & 31u, wid = t >> 5, nw = blockDim.x >> 5;
+  uint32_t const q = base + t;
+  uint32_t key = kSortGroups - 1;
+  if (q < n) {
+    uint32_t const obj = __float_as_uint(w.hit[w.cap + q]);
+    if (obj == UINT32_MAX) {
+      key = 0;
+    } else {
+      const DevScene& S = jobs.scene(J::kMulti ? w.in.job[q] : 0u);
+      uint32_t const type = uint32_t(S.mats[S.objects[obj].mat].type);
+      key = 1u + (type < kSortGroups - 3 ? type : kSortGroups - 3);
+    }
+  }
+  unsigned mine = 0;
+#pragma unroll
+  for (int b = 0; b < kSortGroups; b++) {
+    unsigned const m = __ballot_sync(0xFFFFFFFFu, key == uint32_t(b));
+    if (key == uint32_t(b)) mine = m;
+    if (lane == 0) counts[b][wid] = __popc(m);
+  }
+  __syncthreads();
+  uint32_t pos = __popc(mine & ((1u << lane) - 1u));
+  for (uint32_t b = 0; b < key; b++)
+    for (uint32_t v = 0; v < nw; v++) pos += counts[b][v];
+  for (uint32_t v = 0; v < wid; v++) pos += counts[key][v];
+  perm[pos] = uint16_t(t);
+  __syncthreads();
+  uint32_t const r = base + perm[t];
+  __syncthreads();  // counts and perm are reused by the block's next chunk
+  return r;
+}
+
 // One vertex of Renderer::tracePath (src/renderer.cpp:64-146) for every
 // queued path: emitter hit (73-84), light importance sample with the MIS
 // power heuristic (87-113, its visibility left to the shadow kernel),
@@ -447,7 +491,7 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
   PathBuf const& out = w.out;
   enum : int { kEnd = 0, kEmit = 1, kScatter = 2 };
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    uint32_t const i = base + threadIdx.x;
+    uint32_t const i = material_order(jobs, w, base, n);
     bool const live = i < n;
     uint32_t const jb = (J::kMulti && live) ? in.job[i] : 0u;
     const DevScene& S = jobs.scene(jb);
