@@ -370,6 +370,71 @@ def run_adjoint(device, n_fd=100, reps=3):
             "fd_h1e-3": fd3, "fd_h1e-2": fd2, "workload": ADJ_DESC}
 
 
+LARGE = dict(n_instances=256, width=3840, spp=256, bounces=32, p=0.8)
+LARGE_DESC = ("large: 256 instances of a 65,536-triangle displaced UV sphere (16.8M instanced tris), 2-tri "
+              "ground, 2 quad lights, 3840x2160, 256 spp, 32 bounces, p=0.8, 16 hero wavelengths 400-720 nm "
+              "(80 bins); 16 tile jobs (4x4) of the frame in one batched launch; one adjoint pass (all "
+              "albedo and thin-film IOR spectra, thicknesses, exponents)")
+
+
+def run_large(args):
+    """Config 5: the 4K frame as 16 tile jobs in one batched launch, the
+    same frame as one plain render, and one adjoint pass of it."""
+    import numpy as np
+    import torch
+
+    from lambda_b200 import synth
+    from lambda_b200.renderer import Context
+    from lambda_b200.scene import flatten, load_nls
+    w = dict(LARGE)
+    if args.spp:
+        w["spp"] = args.spp
+    root = os.path.join(tempfile.gettempdir(), "lgpu_bench", "large")
+    nls = synth.instanced(root, n_instances=w["n_instances"], width=w["width"], mesh="uv64k")
+    fs = flatten(load_nls(nls))
+    ctx = Context(0)
+    ctx.upload_many([fs])
+    W, H = ctx.size
+    paths = W * H * w["spp"]
+    d_out = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+    d_tiles = torch.zeros_like(d_out)
+    stream = torch.cuda.current_stream()
+    job = dict(scene=0, spp=w["spp"], max_scatterings=w["bounces"], sample_p=w["p"], seed=3)
+    xs = [W * k // 4 for k in range(5)]
+    ys = [H * k // 4 for k in range(5)]
+    tiles = [dict(job, rect=(xs[a], ys[b], xs[a + 1] - xs[a], ys[b + 1] - ys[b])) for b in range(4)
+             for a in range(4)]
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    t_plain = timed(lambda: ctx.render_device(w["spp"], w["bounces"], w["p"], d_out.data_ptr(), seed=3,
+                                              stream=stream.cuda_stream))
+    t_tiles = timed(lambda: ctx.render_batch_device(tiles, [d_tiles.data_ptr()] * 16, stream=stream.cuda_stream))
+    same = bool(torch.equal(d_out, d_tiles))
+    wimg = torch.from_numpy(np.random.default_rng(5).standard_normal(H * W * 3).astype(np.float32)).cuda()
+    n_spec = int(fs.scene.n_spectra) * int(fs.scene.spec.n_bins)
+    d_gs = torch.zeros(n_spec, dtype=torch.float32, device="cuda")
+    d_gm = torch.zeros(4 * int(fs.scene.n_materials), dtype=torch.float32, device="cuda")
+    t_adj = timed(lambda: ctx.adjoint_device(w["spp"], w["bounces"], w["p"], wimg.data_ptr(), d_gs.data_ptr(),
+                                             d_gm.data_ptr(), seed=3, stream=stream.cuda_stream))
+    line = {"metric": METRIC, "value": paths / t_tiles / 1e6, "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 0, "ms_per_step": t_tiles * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+            "config": {"workload": LARGE_DESC, "paths": paths},
+            "plain_value": paths / t_plain / 1e6, "tiles_identical_to_plain": same,
+            "adjoint_s": t_adj, "adjoint_cost_ratio": t_adj / t_plain,
+            "gradient_nonzero": int((d_gs != 0).sum().item() + (d_gm != 0).sum().item())}
+    print(json.dumps(line))
+    return 0
+
+
 def rmse_check(ctx, w, ref_rows, d_out, stream, oracle_renders=16):
     """Relative RMSE per channel, over the reference's sampled rows, of the
     device image and of the reference's own image at the workload's spp,
@@ -397,8 +462,11 @@ def rmse_check(ctx, w, ref_rows, d_out, stream, oracle_renders=16):
     den = np.sqrt(np.mean(o ** 2, axis=(0, 1)))
     e_g = np.sqrt(np.mean((g - o) ** 2, axis=(0, 1))) / den
     e_c = np.sqrt(np.mean((c - o) ** 2, axis=(0, 1))) / den
+    # means over the rows: a bias between the estimators would show here
+    mean_ratio = np.mean(c, axis=(0, 1)) / np.mean(o, axis=(0, 1))
     return {"device": [float(x) for x in e_g], "reference": [float(x) for x in e_c],
             "ratio": [float(x) for x in e_g / e_c], "rows": len(rows),
+            "reference_mean_over_oracle_mean": [float(x) for x in mean_ratio],
             "oracle": "device, %d spp (%d renders of %d spp with other random streams, FP64 mean)" %
                       (oracle_renders * spp, oracle_renders, spp),
             "what": "relative RMSE per channel (R, G, B) over the reference's sampled rows at %d spp" % spp}
@@ -595,6 +663,8 @@ def main():
     ap.add_argument("--no-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost and FD check")
+    ap.add_argument("--large", action="store_true",
+                    help="the large configuration (4K, 16 tile jobs, one adjoint pass) instead")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="seconds of reference CPU work per sampled step")
     args = ap.parse_args()
@@ -605,6 +675,8 @@ def main():
         w["width"] = args.width
     if args.impl == "reference":
         return run_reference(args, w)
+    if args.large:
+        return run_large(args)
     return run_device(args, w)
 
 

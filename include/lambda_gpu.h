@@ -277,12 +277,17 @@ int lgpu_upload_scenes(lgpu_ctx* ctx, const lgpu_scene* const* scenes, uint32_t 
 
 /* One job of a batched render: a slot of the scene table, the settings of
    Renderer::render for it, and its output (that scene's
-   cam.width*cam.height*3 floats of linear RGB, row 0 at the top). */
+   cam.width*cam.height*3 floats of linear RGB, row 0 at the top).  A job
+   may cover a rectangle of the frame (x0, y0 from the top-left corner of the
+   output, width x height pixels; width 0 = the whole frame): it then writes
+   only those pixels of `out`, with the values a render of the whole frame
+   gives them, so tile jobs of one frame can share one output. */
 typedef struct lgpu_job {
   uint32_t scene;
   uint32_t reserved;
   lgpu_render_params params;
   float* out;
+  uint32_t x0, y0, width, height;
 } lgpu_job;
 
 /* Renders n jobs in one streaming wavefront: paths of all jobs share the

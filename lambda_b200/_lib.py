@@ -99,7 +99,9 @@ class RenderParams(ctypes.Structure):
 
 class Job(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
-                ("params", RenderParams), ("out", ctypes.c_void_p)]
+                ("params", RenderParams), ("out", ctypes.c_void_p),
+                ("x0", ctypes.c_uint32), ("y0", ctypes.c_uint32), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32)]
 
 
 class WaveConfig(ctypes.Structure):

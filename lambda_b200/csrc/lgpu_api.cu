@@ -258,8 +258,8 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
 
 // paths in flight: about 2^21, fewer for small renders
 constexpr uint64_t kQueueCap = uint64_t(1) << 21;
-// the (sample, pixel) film buffer of one chunk stays under 2 GiB
-constexpr uint64_t kSbufBytes = uint64_t(1) << 31;
+// the (sample, pixel) film buffer of one chunk stays under 8 GiB (of 180)
+constexpr uint64_t kSbufBytes = uint64_t(1) << 33;
 
 // Sizes the wavefront buffers for npix pixels, n_items work items in chunks
 // of chunk_items, and fills ws.
@@ -341,6 +341,29 @@ int render_impl(lgpu_ctx* ctx, const lgpu_render_params* p, float* d_out, cudaSt
   return render_scene(ctx, ctx->S, p, d_out, st);
 }
 
+// The rectangle of a job in scene rows (x0, first scene row, width,
+// height); false if it does not fit the frame.
+bool job_rect(const lgpu_job& j, const lgpu_camera& c, uint32_t& x0, uint32_t& row0, uint32_t& w, uint32_t& h) {
+  uint32_t const W = uint32_t(c.width), H = uint32_t(c.height);
+  if (j.width == 0) {
+    x0 = 0;
+    row0 = 0;
+    w = W;
+    h = H;
+    return true;
+  }
+  if (j.height == 0 || j.x0 >= W || j.y0 >= H || j.width > W - j.x0 || j.height > H - j.y0) return false;
+  x0 = j.x0;
+  w = j.width;
+  h = j.height;
+  row0 = H - j.y0 - j.height;  // output rows count from the top, scene rows from the bottom
+  return true;
+}
+
+bool full_frame(const lgpu_job& j, const lgpu_camera& c) {
+  return j.width == 0 || (j.x0 == 0 && j.y0 == 0 && j.width == uint32_t(c.width) && j.height == uint32_t(c.height));
+}
+
 int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_outs, cudaStream_t st);
 
 // A batch split by the megakernel threshold: the small jobs render with the
@@ -398,16 +421,21 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
     if (jobs[k].params.spp == 0)
       return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": spp must be >= 1");
     if (!d_outs[k]) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": null output");
+    uint32_t x0, r0, tw, th;
+    if (!job_rect(jobs[k], ctx->slots[jobs[k].scene].S.cam, x0, r0, tw, th))
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": rectangle outside the frame");
     timing = timing || (jobs[k].params.flags & LGPU_FLAG_KERNEL_TIMING);
     linear = linear || (jobs[k].params.flags & LGPU_FLAG_REFERENCE_ORDER);
   }
-  if (n == 1) return render_scene(ctx, ctx->slots[jobs[0].scene].S, &jobs[0].params, d_outs[0], st);
-  // jobs below the megakernel threshold run on the side stream
+  if (n == 1 && full_frame(jobs[0], ctx->slots[jobs[0].scene].S.cam))
+    return render_scene(ctx, ctx->slots[jobs[0].scene].S, &jobs[0].params, d_outs[0], st);
+  // whole-frame jobs below the megakernel threshold run on the side stream
   std::vector<uint32_t> wave_jobs, mega_jobs;
   for (uint32_t k = 0; k < n; k++) {
     const lgpu_camera& c = ctx->slots[jobs[k].scene].S.cam;
     uint64_t const items = uint64_t(c.width) * c.height * jobs[k].params.spp;
-    ((ctx->cfg.mega_items && items < ctx->cfg.mega_items) ? mega_jobs : wave_jobs).push_back(k);
+    bool const mega = ctx->cfg.mega_items && items < ctx->cfg.mega_items && full_frame(jobs[k], c);
+    (mega ? mega_jobs : wave_jobs).push_back(k);
   }
   if (!mega_jobs.empty()) return batch_split(ctx, jobs, n, d_outs, st, wave_jobs, mega_jobs);
   std::vector<DevJob> hj(n);
@@ -418,7 +446,9 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
     DevJob& d = hj[k];
     d.S = ctx->slots[jobs[k].scene].S;
     d.a = render_args(&jobs[k].params, d.S);
-    d.npix = d.a.pixel_count;
+    uint32_t th = 0;
+    job_rect(jobs[k], d.S.cam, d.col0, d.row0, d.tile_w, th);
+    d.npix = d.tile_w * th;
     d.item_base = g;
     d.pix_base = uint32_t(px);
     d.out = d_outs[k];
@@ -475,7 +505,7 @@ int adjoint_impl(lgpu_ctx* ctx, const lgpu_render_params* p, const float* d_dimg
   uint64_t const n_items = npix * a.spp;
   // per work item of a chunk: 12 B film entry, 4K B radiance, 8 B visibility
   uint64_t const per_item = 12 + 4ull * S.hero_k + 8;
-  uint64_t const max_items = (uint64_t(1) << 32) / per_item;
+  uint64_t const max_items = (uint64_t(1) << 34) / per_item;
   uint64_t const chunk = n_items < max_items ? n_items : max_items;
   WaveState ws{};
   if (int r = ensure_wave(ctx, a.pixel_count, n_items, chunk, false, ws, true)) return r;
@@ -748,9 +778,16 @@ int lgpu_render_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n) {
   for (uint32_t k = 0; k < n; k++) outs[k] = ctx->batch_out.ptr + off[k];
   int const rc = batch_impl(ctx, jobs, n, outs.data(), ctx->stream);
   if (rc != LGPU_OK) return rc;
-  for (uint32_t k = 0; k < n && e == cudaSuccess; k++)
-    e = cudaMemcpyAsync(jobs[k].out, outs[k], (off[k + 1] - off[k]) * sizeof(float), cudaMemcpyDeviceToHost,
-                        ctx->stream);
+  // each job's rectangle of its frame (tile jobs may share a host output)
+  for (uint32_t k = 0; k < n && e == cudaSuccess; k++) {
+    const lgpu_camera& c = ctx->slots[jobs[k].scene].S.cam;
+    uint32_t x0, r0, tw, th;
+    job_rect(jobs[k], c, x0, r0, tw, th);
+    size_t const pitch = size_t(c.width) * 3 * sizeof(float);
+    size_t const first = (size_t(c.height - r0 - th) * c.width + x0) * 3;
+    e = cudaMemcpy2DAsync(jobs[k].out + first, pitch, outs[k] + first, pitch, size_t(tw) * 3 * sizeof(float), th,
+                          cudaMemcpyDeviceToHost, ctx->stream);
+  }
   if (e != cudaSuccess) return cuda_fail(ctx, e, "batch readback");
   return collect(ctx, "render batch", batch_timing(jobs, n));
 }

@@ -216,6 +216,22 @@ struct TravStats {
   uint32_t insts;  // object (instance) tests
 };
 
+// Position of each hit child in the far-to-near order: d goes before c when
+// t[d] > t[c], or t[d] == t[c] and d < c.  One comparison per pair; a miss
+// has t = 0, below every hit, so it does not shift a hit's rank.
+__device__ __forceinline__ void child_ranks(const float (&t)[8], int (&rank)[8]) {
+#pragma unroll
+  for (int c = 0; c < 8; c++) rank[c] = 0;
+#pragma unroll
+  for (int c = 1; c < 8; c++)
+#pragma unroll
+    for (int d = 0; d < c; d++) {
+      bool const d_first = t[d] >= t[c];
+      rank[c] += d_first ? 1 : 0;
+      rank[d] += d_first ? 0 : 1;
+    }
+}
+
 // Tests the children of an interior node and pushes the hit ones so that
 // the nearest is on top; equal distances keep child order, as the
 // reference's insertion-sorted std::sort of <= 8 elements does
@@ -234,19 +250,11 @@ __device__ __forceinline__ bool push_children(const WideNode& nd, const Ray& r, 
 #pragma unroll
   for (int c = 0; c < 8; c++) hits += (t[c] != 0.f) ? 1 : 0;
   if (sp + hits > cap) return false;
+  int rank[8];
+  child_ranks(t, rank);
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    if (t[c] == 0.f) continue;
-    // position in the far-to-near order among the hit children
-    int rank = 0;
-#pragma unroll
-    for (int d = 0; d < 8; d++) {
-      if (d == c || t[d] == 0.f) continue;
-      bool const before = (t[d] > t[c]) || (t[d] == t[c] && d < c);
-      rank += before ? 1 : 0;
-    }
-    stack[sp + rank] = StackEntry{ref[c], t[c]};
-  }
+  for (int c = 0; c < 8; c++)
+    if (t[c] != 0.f) stack[sp + rank[c]] = StackEntry{ref[c], t[c]};
   sp += hits;
   return true;
 }

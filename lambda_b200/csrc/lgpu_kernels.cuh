@@ -168,9 +168,10 @@ struct DevJob {
   DevScene S;
   RenderArgs a;
   uint64_t item_base;  // first work item of the job
-  uint32_t npix;
+  uint32_t npix;       // pixels of its rectangle
   uint32_t pix_base;   // first pixel of the job in the batch film
-  float* out;          // linear RGB, width*height*3, row 0 at the top
+  float* out;          // linear RGB of the whole frame, width*height*3, row 0 at the top
+  uint32_t col0, row0, tile_w;  // rectangle: first column, first scene row, width
 };
 
 #ifdef __CUDACC__
@@ -191,6 +192,8 @@ struct OneJob {
   __device__ __forceinline__ uint32_t pix_base(uint32_t) const { return 0; }
   __device__ __forceinline__ uint32_t npix_of(uint32_t) const { return npix; }
   __device__ __forceinline__ float* out_of(uint32_t) const { return out; }
+  // frame pixel (scene row-major) of the job's local pixel
+  __device__ __forceinline__ uint32_t frame_pixel(uint32_t, uint32_t p) const { return p; }
 };
 
 struct JobTable {
@@ -224,6 +227,11 @@ struct JobTable {
   __device__ __forceinline__ uint32_t pix_base(uint32_t j) const { return pix_bases[j]; }
   __device__ __forceinline__ uint32_t npix_of(uint32_t j) const { return d[j].npix; }
   __device__ __forceinline__ float* out_of(uint32_t j) const { return d[j].out; }
+  __device__ __forceinline__ uint32_t frame_pixel(uint32_t j, uint32_t p) const {
+    const DevJob& jb = d[j];
+    uint32_t const r = p / jb.tile_w;
+    return (jb.row0 + r) * uint32_t(jb.S.cam.width) + jb.col0 + (p - r * jb.tile_w);
+  }
 };
 #endif
 

@@ -61,18 +61,11 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
       if (t[c] != 0.f) st.push(StackEntry{ref[c], t[c]});
     return true;
   }
+  int rank[8];
+  child_ranks(t, rank);
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    if (t[c] == 0.f) continue;
-    int rank = 0;
-#pragma unroll
-    for (int d = 0; d < 8; d++) {
-      if (d == c || t[d] == 0.f) continue;
-      bool const before = (t[d] > t[c]) || (t[d] == t[c] && d < c);
-      rank += before ? 1 : 0;
-    }
-    st.at(st.sp + rank) = StackEntry{ref[c], t[c]};
-  }
+  for (int c = 0; c < 8; c++)
+    if (t[c] != 0.f) st.at(st.sp + rank[c]) = StackEntry{ref[c], t[c]};
   st.sp += hits;
   return true;
 }

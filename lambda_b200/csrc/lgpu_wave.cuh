@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) wf_generate_stream(J jobs, WaveState w, D
     uint32_t const npix = jobs.npix_of(jb);
     uint64_t const l = g - jobs.item_base(jb);
     uint32_t const sample = uint32_t(l / npix);
-    uint32_t const pix = uint32_t(l - uint64_t(sample) * npix);
+    uint32_t const pix = jobs.frame_pixel(jb, uint32_t(l - uint64_t(sample) * npix));
     uint32_t const p = pos + k;
     float const omega = S.lambda_sup - S.lambda_inf;
     const lgpu_camera& C = S.cam;
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(256) wf_finalize(J jobs, WaveState w) {
   for (uint32_t gp = blockIdx.x * blockDim.x + threadIdx.x; gp < w.npix; gp += gridDim.x * blockDim.x) {
     uint32_t const jb = jobs.job_of_pixel(gp);
     const DevScene& S = jobs.scene(jb);
-    uint32_t const pix = gp - jobs.pix_base(jb);
+    uint32_t const pix = jobs.frame_pixel(jb, gp - jobs.pix_base(jb));
     uint32_t const W = uint32_t(S.cam.width), H = uint32_t(S.cam.height);
     uint32_t const i = pix / W, j = pix - i * W;
     float const norm = float(jobs.args(jb).spp) * float(K);

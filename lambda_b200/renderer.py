@@ -95,6 +95,8 @@ class Context:
                                            seed=int(j.get("seed", 0)),
                                            spp_offset=int(j.get("spp_offset", 0)))
             arr[k].out = o
+            if "rect" in j:  # (x0, y0, width, height) from the top-left of the frame
+                arr[k].x0, arr[k].y0, arr[k].width, arr[k].height = (int(v) for v in j["rect"])
         return arr
 
     def wave_config(self):
@@ -121,14 +123,15 @@ class Context:
 
     def render_batch(self, jobs):
         """Renders every job (dicts: scene, spp, max_scatterings, sample_p
-        and optionally seed, flags, spp_offset) in one batched launch;
-        returns one (height, width, 3) image per job."""
+        and optionally seed, flags, spp_offset, rect = (x0, y0, width,
+        height)) in one batched launch; returns one (height, width, 3) frame
+        per job (a rect job fills only its rectangle; the rest is zero)."""
         imgs = []
         for j in jobs:
             s = int(j["scene"])
             # an unknown slot gets a placeholder; the library rejects the job
             w, h = self.slot_size(s) if 0 <= s < len(self.flats) else (1, 1)
-            imgs.append(np.empty((h, w, 3), np.float32))
+            imgs.append(np.zeros((h, w, 3), np.float32))
         arr = self._jobs(jobs, [im.ctypes.data for im in imgs])
         L.check(self.h, self._lib.lgpu_render_batch(self.h, arr, len(jobs)), "render_batch")
         return imgs

@@ -245,6 +245,17 @@ def displaced_icosphere(subdiv, seed, amp=0.05, freq=3.0):
     """Icosphere displaced along its normal by amp * Perlin(freq * p); vertex
     normals are area-weighted face normals of the displaced surface."""
     V, F = icosphere(subdiv)
+    return _displace(V, F, seed, amp, freq)
+
+
+def displaced_uv_sphere(seed, n_lon=256, n_lat=129, amp=0.05, freq=3.0):
+    """UV sphere of n_lon * (n_lat - 2) * 2 + 2 * n_lon triangles (65,536 by
+    default) displaced as displaced_icosphere."""
+    V, _, F = uv_sphere(n_lon, n_lat)
+    return _displace(V, F, seed, amp, freq)
+
+
+def _displace(V, F, seed, amp, freq):
     rng = np.random.default_rng(seed)
     perm = rng.permutation(256)
     n = perlin3(V * freq + rng.uniform(0, 100, size=3), perm)
@@ -338,15 +349,23 @@ def mixed(out_dir, width=96, ar=1.25, lights=("sphere", "quaddir", "point"), see
     return path
 
 
-def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 9):
-    """Writes the instanced scene; returns the .nls path."""
+def instanced(out_dir, n_instances=64, subdiv=7, seed=1234, width=1920, ar=16 / 9, mesh="icosphere"):
+    """Writes the instanced scene; returns the .nls path.  mesh: "icosphere"
+    (subdivision subdiv) or "uv64k" (the 65,536-triangle displaced UV
+    sphere)."""
     os.makedirs(out_dir, exist_ok=True)
     d = os.path.abspath(out_dir)
     rng = np.random.default_rng(seed)
-    mesh_path = os.path.join(d, f"icosphere_s{subdiv}_seed{seed}.obj")
-    if not os.path.exists(mesh_path):
-        V, N, F = displaced_icosphere(subdiv, seed)
-        write_indexed_obj(mesh_path, V, N, F)
+    if mesh == "uv64k":
+        mesh_path = os.path.join(d, f"uvsphere64k_seed{seed}.obj")
+        if not os.path.exists(mesh_path):
+            V, N, F = displaced_uv_sphere(seed)
+            write_indexed_obj(mesh_path, V, N, F)
+    else:
+        mesh_path = os.path.join(d, f"icosphere_s{subdiv}_seed{seed}.obj")
+        if not os.path.exists(mesh_path):
+            V, N, F = displaced_icosphere(subdiv, seed)
+            write_indexed_obj(mesh_path, V, N, F)
     # written at z = 1, moved to z = 0 by the object transform (flat bounds
     # through the dummy vertex are never hit, see _write_flat_mesh)
     _write_flat_mesh(os.path.join(d, "ground.obj"),

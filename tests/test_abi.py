@@ -37,7 +37,7 @@ def test_struct_sizes_match_c():
     assert ctypes.sizeof(L.Scene) == 192
     assert ctypes.sizeof(L.RenderParams) == 32
     assert ctypes.sizeof(L.Hit) == 56
-    assert ctypes.sizeof(L.Job) == 48
+    assert ctypes.sizeof(L.Job) == 64
 
 
 def test_errors_without_arguments():

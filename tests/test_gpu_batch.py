@@ -127,3 +127,24 @@ def test_megakernel_split_and_autotune(scenes):
     again = ctx.render_batch(JOBS)
     for a, b in zip(again, ref):
         assert np.array_equal(a, b)
+
+
+def test_tile_jobs_compose_the_frame(scenes):
+    """Jobs covering rectangles of one frame (uneven split) give exactly the
+    pixels of the whole-frame render."""
+    ctx = Context()
+    ctx.upload_many(scenes)
+    w, h = ctx.slot_size(1)
+    base = dict(scene=1, spp=4, max_scatterings=6, sample_p=0.8, seed=9)
+    full = ctx.render_batch([base, JOBS[0]])[0]
+    xs, ys = [0, w // 3, w], [0, h // 2 + 1, h]
+    tiles = [dict(base, rect=(xs[a], ys[b], xs[a + 1] - xs[a], ys[b + 1] - ys[b]))
+             for a in range(2) for b in range(2)]
+    imgs = ctx.render_batch(tiles)
+    got = np.zeros_like(full)
+    for t, im in zip(tiles, imgs):
+        x0, y0, tw, th = t["rect"]
+        got[y0:y0 + th, x0:x0 + tw] = im[y0:y0 + th, x0:x0 + tw]
+    assert np.array_equal(got, full)
+    with pytest.raises(L.LgpuError):
+        ctx.render_batch([dict(base, rect=(w - 2, 0, 4, 4)), JOBS[0]])
