@@ -193,13 +193,46 @@ __device__ __forceinline__ float child_box_t(const WideNode& nd, int c, const Ra
   float const dminz = ml(sb(bminz, r.p.z), r.inv.z);
   float const dmaxz = ml(sb(bmaxz, r.p.z), r.inv.z);
   float tmin = kBias, tmax = t_max;
-  tmin = dminx > tmin ? dminx : tmin;
-  tmax = dmaxx < tmax ? dmaxx : tmax;
-  tmin = dminy > tmin ? dminy : tmin;
-  tmax = dmaxy < tmax ? dmaxy : tmax;
-  tmin = dminz > tmin ? dminz : tmin;
-  tmax = dmaxz < tmax ? dmaxz : tmax;
+  // no slab value is NaN (inv is finite or ±FLT_MAX, b - p is finite) and a
+  // ±0 never decides a hit (tmin starts at kBias > 0), so fmaxf/fminf
+  // return what the reference's compare-and-select does
+  tmin = fmaxf(fmaxf(fmaxf(tmin, dminx), dminy), dminz);
+  tmax = fminf(fminf(fminf(tmax, dmaxx), dmaxy), dmaxz);
   return tmin <= tmax ? tmin : 0.f;
+}
+
+// All 8 child boxes of a wide node at once (the results of child_box_t):
+// the near and far plane rows of each axis are chosen once from the signs
+// of the ray's direction and read as float4.  No slab value is NaN (inv is
+// finite or ±FLT_MAX, b - p is finite) and a ±0 never decides a hit (tmin
+// starts at kBias > 0), so fmaxf/fminf return what the reference's
+// compare-and-select does.
+__device__ __forceinline__ void node_boxes_t(const WideNode& nd, const Ray& r, float t_max, float (&t)[8]) {
+  bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
+  const float4* const nrx = reinterpret_cast<const float4*>(nx ? nd.hix : nd.lox);
+  const float4* const frx = reinterpret_cast<const float4*>(nx ? nd.lox : nd.hix);
+  const float4* const nry = reinterpret_cast<const float4*>(ny ? nd.hiy : nd.loy);
+  const float4* const fry = reinterpret_cast<const float4*>(ny ? nd.loy : nd.hiy);
+  const float4* const nrz = reinterpret_cast<const float4*>(nz ? nd.hiz : nd.loz);
+  const float4* const frz = reinterpret_cast<const float4*>(nz ? nd.loz : nd.hiz);
+  // four children at a time: the six float4 of a half and their tests
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    float4 const a = nrx[h], b = frx[h], c = nry[h], d = fry[h], e = nrz[h], f = frz[h];
+    float const bnx[4] = {a.x, a.y, a.z, a.w}, bfx[4] = {b.x, b.y, b.z, b.w};
+    float const bny[4] = {c.x, c.y, c.z, c.w}, bfy[4] = {d.x, d.y, d.z, d.w};
+    float const bnz[4] = {e.x, e.y, e.z, e.w}, bfz[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      float const tmin =
+          fmaxf(fmaxf(fmaxf(kBias, ml(sb(bnx[k], r.p.x), r.inv.x)), ml(sb(bny[k], r.p.y), r.inv.y)),
+                ml(sb(bnz[k], r.p.z), r.inv.z));
+      float const tmax =
+          fminf(fminf(fminf(t_max, ml(sb(bfx[k], r.p.x), r.inv.x)), ml(sb(bfy[k], r.p.y), r.inv.y)),
+                ml(sb(bfz[k], r.p.z), r.inv.z));
+      t[4 * h + k] = tmin <= tmax ? tmin : 0.f;
+    }
+  }
 }
 
 struct StackEntry {

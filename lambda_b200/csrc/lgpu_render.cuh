@@ -269,7 +269,10 @@ cudaError_t wave_chunk(const J& jobs, WaveState& w, uint64_t c0, uint32_t total,
     launch_closest<K>(jobs, wi, g, linear, c_closest, st);
     run->end(0, st);
     run->begin(2, st);
-    wf_shade<K, J><<<g.shade, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
+    // one block per queue chunk, not persistent: a block's warps finish
+    // their material-sorted groups at different times, and a persistent
+    // block would hold the fast ones at the next chunk's sort barrier
+    wf_shade<K, J><<<(wi.cap + g.shade_block - 1) / g.shade_block, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
     run->end(2, st);
     run->begin(1, st);
     if (linear) wf_shadow<K, J><<<g.shadow, 128, kTraceSmem, st>>>(jobs, wi, c_shadow);

@@ -41,15 +41,28 @@ constexpr int kSplitCap = kSmemStack + kLocalStack;
 // push_children (lgpu_intersect.cuh) writing through a SplitStack.  With
 // `sorted` false (any-hit queries, whose boolean answer does not depend on
 // the visiting order) the hit children are pushed in child order.
+template <bool ROWS>
 __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ray& r, float t_max,
                                                     SplitStack& st, bool sorted) {
-  bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
   float t[8];
   uint32_t ref[8];
+  // ROWS: the row-wise test, faster where registers allow it (the shadow
+  // kernel); the closest-hit kernel keeps the per-child test, which leaves
+  // registers for the sorted push (both give the same t)
+  if (ROWS) {
+    node_boxes_t(nd, r, t_max, t);
 #pragma unroll
-  for (int c = 0; c < 8; c++) {
-    ref[c] = nd.child[c];
-    t[c] = (ref[c] != kEmptyChild) ? child_box_t(nd, c, r, nx, ny, nz, t_max) : 0.f;
+    for (int c = 0; c < 8; c++) {
+      ref[c] = nd.child[c];
+      if (ref[c] == kEmptyChild) t[c] = 0.f;
+    }
+  } else {
+    bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      ref[c] = nd.child[c];
+      t[c] = (ref[c] != kEmptyChild) ? child_box_t(nd, c, r, nx, ny, nz, t_max) : 0.f;
+    }
   }
   int hits = 0;
 #pragma unroll
@@ -97,7 +110,7 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
     if (e.t > h.z) continue;
     if (!(e.ref & kLeafBit)) {
       ts.nodes++;
-      if (!push_children_split(S.nodes[e.ref], in_mesh ? l : w, h.z, st, !ANY)) {
+      if (!push_children_split<ANY>(S.nodes[e.ref], in_mesh ? l : w, h.z, st, !ANY)) {
         ts.flags |= 1u;
         break;
       }
@@ -241,7 +254,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   if (e.t > h.z) return st.sp == 0;
   if (!(e.ref & kLeafBit)) {
     ts.nodes++;
-    if (!push_children_split(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
+    if (!push_children_split<ANY>(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
       ts.flags |= 1u;
       return true;
     }
