@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(128) wf_shade_adjoint(OneJob jobs, WaveState w
   float const omega = S.lambda_sup - S.lambda_inf;
   float const step = omega / float(K);
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    uint32_t const i = base + threadIdx.x;
+    uint32_t const i = material_order(jobs, w, base, n);
     bool const live = i < n;
     bool cont = false, scatter = false, visible = false;
     f3 np = f3{0.f, 0.f, 0.f}, nd = f3{0.f, 0.f, 1.f};
@@ -357,11 +357,8 @@ __global__ void __launch_bounds__(128) wf_shade_adjoint(OneJob jobs, WaveState w
 template <int K>
 cudaError_t replay_chunk(const OneJob& jobs, WaveState& w, uint64_t c0, uint32_t total, bool linear,
                          const AdjointArgs& g, DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
-  static uint32_t gen_per_sm = 0, shade_per_sm = 0;
-  if (!gen_per_sm) {
-    gen_per_sm = blocks_per_sm(wf_replay_generate<K>, 256, 0);
-    shade_per_sm = blocks_per_sm(wf_shade_adjoint<K>, 128, 0);
-  }
+  static uint32_t gen_per_sm = 0;
+  if (!gen_per_sm) gen_per_sm = blocks_per_sm(wf_replay_generate<K>, 256, 0);
   WaveGrids const gr = wave_grids<K, OneJob>(run->cfg);
   uint32_t const sms = wave_occupancy<K, OneJob>().sms;
   DevCounters* const c_closest = run->on ? d_cnt + 1 : d_cnt;
@@ -375,7 +372,8 @@ cudaError_t replay_chunk(const OneJob& jobs, WaveState& w, uint64_t c0, uint32_t
     launch_closest<K>(jobs, wi, gr, linear, c_closest, st);
     run->end(0, st);
     run->begin(2, st);
-    wf_shade_adjoint<K><<<sms * shade_per_sm, 128, 0, st>>>(jobs, wi, g);
+    // one block per queue chunk (see wave_chunk)
+    wf_shade_adjoint<K><<<(wi.cap + 127) / 128, 128, 0, st>>>(jobs, wi, g);
     run->end(2, st);
     // plan, generate, trace (+ fallback), shade
     run->total += linear ? 4 : 5;

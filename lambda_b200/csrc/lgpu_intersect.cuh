@@ -232,6 +232,9 @@ __device__ __forceinline__ void node_boxes_t(const WideNode& nd, const Ray& r, f
                 ml(sb(bfz[k], r.p.z), r.inv.z));
       t[4 * h + k] = tmin <= tmax ? tmin : 0.f;
     }
+    // keeps the second half's loads after the first half's tests (fewer
+    // live registers)
+    asm volatile("" ::: "memory");
   }
 }
 

@@ -46,9 +46,8 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
                                                     SplitStack& st, bool sorted) {
   float t[8];
   uint32_t ref[8];
-  // ROWS: the row-wise test, faster where registers allow it (the shadow
-  // kernel); the closest-hit kernel keeps the per-child test, which leaves
-  // registers for the sorted push (both give the same t)
+  // ROWS: the row-wise test (the persistent kernels, which have the
+  // registers for it); otherwise the per-child test (both give the same t)
   if (ROWS) {
     node_boxes_t(nd, r, t_max, t);
 #pragma unroll
@@ -254,7 +253,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   if (e.t > h.z) return st.sp == 0;
   if (!(e.ref & kLeafBit)) {
     ts.nodes++;
-    if (!push_children_split<ANY>(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
+    if (!push_children_split<true>(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
       ts.flags |= 1u;
       return true;
     }

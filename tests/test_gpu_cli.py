@@ -1,0 +1,121 @@
+"""The reference's own `lambda` CLI with Renderer::render replaced by the
+C-ABI drop-in (lambda_b200/host/renderer_gpu.cpp, built by
+lambda_b200/host/Makefile): it renders a scene file end to end and its raw
+PNG equals the 8-bit encode of the Python host's render of the same scene
+with the same settings and seed."""
+import json
+import os
+import shutil
+import struct
+import subprocess
+import zlib
+
+import numpy as np
+import pytest
+
+from lambda_b200 import synth
+from lambda_b200.renderer import Context, Rendering
+from lambda_b200.scene import load_nls
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(REPO, "lambda_b200", "host", "_build", "lambda")
+
+
+def read_png_rgb(path):
+    """8-bit RGB PNG (non-interlaced) -> (h, w, 3) uint8."""
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, idat = 8, b""
+    w = h = None
+    while pos < len(data):
+        n = struct.unpack(">I", data[pos:pos + 4])[0]
+        kind = data[pos + 4:pos + 8]
+        body = data[pos + 8:pos + 8 + n]
+        if kind == b"IHDR":
+            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
+            assert depth == 8 and ctype == 2
+        elif kind == b"IDAT":
+            idat += body
+        pos += 12 + n
+    raw = zlib.decompress(idat)
+    stride = 3 * w
+    out = np.zeros((h, stride), np.int32)
+    prev = np.zeros(stride, np.int32)
+    for y in range(h):
+        f = raw[y * (stride + 1)]
+        row = np.frombuffer(raw, np.uint8, stride, y * (stride + 1) + 1).astype(np.int32)
+        cur = np.zeros(stride, np.int32)
+        for x in range(stride):
+            a = cur[x - 3] if x >= 3 else 0
+            b = prev[x]
+            c = prev[x - 3] if x >= 3 else 0
+            if f == 0:
+                p = 0
+            elif f == 1:
+                p = a
+            elif f == 2:
+                p = b
+            elif f == 3:
+                p = (a + b) // 2
+            else:
+                pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
+                p = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
+            cur[x] = (row[x] + p) & 255
+        out[y] = cur
+        prev = cur
+    return out.reshape(h, w, 3).astype(np.uint8)
+
+
+def cmf_files(dst):
+    """The CMF tables the reference reads at start-up (cg.hpp:329-337),
+    written back from the verbatim entries in lambda_b200/data."""
+    d = json.load(open(os.path.join(REPO, "lambda_b200", "data", "cie_tables.json")))
+    os.makedirs(dst, exist_ok=True)
+    for axis in "xyz":
+        with open(os.path.join(dst, "xyz_%s.csv" % axis), "w") as f:
+            f.write("".join("%s,%s\n" % (a, b) for a, b in d["cmf_" + axis]))
+    with open(os.path.join(dst, "cie1931-basis-bt709-380+5+780.csv"), "w") as f:
+        f.write("".join(",".join(r) + "\n" for r in d["bt709_basis"]["rows"]))
+
+
+@pytest.mark.gpu
+def test_reference_cli_renders_on_the_gpu(tmp_path):
+    if not os.path.exists(CLI):
+        pytest.skip("the CLI was not built (make -C lambda_b200/host needs the reference sources)")
+    root = tmp_path / "root"
+    cmf_files(str(root / "lib" / "numli" / "data"))
+    bin_dir = root / "bin"
+    (bin_dir / "scenes").mkdir(parents=True)
+    (bin_dir / "render").mkdir()
+    nls = synth.mixed(str(tmp_path / "mixed_cli"), width=48)
+    shutil.copy(nls, bin_dir / "scenes" / "mixed.nls")
+    r = subprocess.run([CLI, "scenes/mixed.nls", "-s", "16", "-b", "8", "-p", "0.8"], cwd=str(bin_dir),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    raw = read_png_rgb(str(bin_dir / "render" / "mixed-16spp-8b-0.80p-raw.png"))
+    ctx = Context()
+    ctx.upload(load_nls(nls))
+    img = ctx.render(16, 8, 0.8, seed=0)
+    assert np.array_equal(raw, Rendering(img).rgb24())
+
+
+def test_reference_cli_fails_loudly_without_a_device(tmp_path):
+    """Without a CUDA device the drop-in render raises (the reference's CLI
+    does not catch it): no silent CPU fallback."""
+    if not os.path.exists(CLI):
+        pytest.skip("the CLI was not built (make -C lambda_b200/host needs the reference sources)")
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    root = tmp_path / "root"
+    cmf_files(str(root / "lib" / "numli" / "data"))
+    bin_dir = root / "bin"
+    (bin_dir / "scenes").mkdir(parents=True)
+    (bin_dir / "render").mkdir()
+    nls = synth.mixed(str(tmp_path / "mixed_cli"), width=16)
+    shutil.copy(nls, bin_dir / "scenes" / "mixed.nls")
+    r = subprocess.run([CLI, "scenes/mixed.nls", "-s", "1"], cwd=str(bin_dir), capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode != 0
+    assert "no CUDA device" in r.stderr + r.stdout
+    assert not os.listdir(bin_dir / "render")
