@@ -22,33 +22,38 @@ CLI = os.path.join(REPO, "lambda_b200", "host", "_build", "lambda")
 
 
 def read_png_rgb(path):
-    """8-bit RGB PNG (non-interlaced) -> (h, w, 3) uint8."""
+    """A non-interlaced PNG (lodepng picks the smallest colour type: grey,
+    RGB, palette, with or without alpha) -> (h, w, 3) uint8."""
     data = open(path, "rb").read()
     assert data[:8] == b"\x89PNG\r\n\x1a\n"
-    pos, idat = 8, b""
-    w = h = None
+    pos, idat, plte = 8, b"", None
     while pos < len(data):
         n = struct.unpack(">I", data[pos:pos + 4])[0]
         kind = data[pos + 4:pos + 8]
         body = data[pos + 8:pos + 8 + n]
         if kind == b"IHDR":
-            w, h, depth, ctype = struct.unpack(">IIBB", body[:10])
-            assert depth == 8 and ctype == 2
+            w, h, depth, ctype, _, _, interlace = struct.unpack(">IIBBBBB", body[:13])
+            assert interlace == 0
+        elif kind == b"PLTE":
+            plte = np.frombuffer(body, np.uint8).reshape(-1, 3)
         elif kind == b"IDAT":
             idat += body
         pos += 12 + n
+    channels = {0: 1, 2: 3, 3: 1, 4: 2, 6: 4}[ctype]
+    bits = channels * depth
+    stride = (w * bits + 7) // 8
+    bpp = max(1, bits // 8)
     raw = zlib.decompress(idat)
-    stride = 3 * w
-    out = np.zeros((h, stride), np.int32)
+    rows = np.zeros((h, stride), np.uint8)
     prev = np.zeros(stride, np.int32)
     for y in range(h):
         f = raw[y * (stride + 1)]
         row = np.frombuffer(raw, np.uint8, stride, y * (stride + 1) + 1).astype(np.int32)
         cur = np.zeros(stride, np.int32)
         for x in range(stride):
-            a = cur[x - 3] if x >= 3 else 0
+            a = cur[x - bpp] if x >= bpp else 0
             b = prev[x]
-            c = prev[x - 3] if x >= 3 else 0
+            c = prev[x - bpp] if x >= bpp else 0
             if f == 0:
                 p = 0
             elif f == 1:
@@ -61,9 +66,21 @@ def read_png_rgb(path):
                 pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
                 p = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
             cur[x] = (row[x] + p) & 255
-        out[y] = cur
+        rows[y] = cur
         prev = cur
-    return out.reshape(h, w, 3).astype(np.uint8)
+    if depth < 8:  # packed palette or grey indices
+        vals = np.unpackbits(rows, axis=1).reshape(h, -1, depth)[:, :w]
+        vals = (vals * (1 << np.arange(depth - 1, -1, -1))).sum(axis=2)
+    else:
+        assert depth == 8
+        vals = rows.reshape(h, w, channels)
+    if ctype == 3:
+        return plte[vals]
+    if ctype in (0, 4):
+        # grey below 8 bits is scaled to the full byte range
+        g = vals * (255 // ((1 << depth) - 1)) if depth < 8 else vals[..., 0]
+        return np.repeat(g[..., None], 3, axis=2).astype(np.uint8)
+    return vals[..., :3].astype(np.uint8)
 
 
 def cmf_files(dst):
