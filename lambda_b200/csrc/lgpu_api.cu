@@ -461,7 +461,9 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
   }
   items[n] = g;
   pixels[n] = uint32_t(px);
-  uint64_t const max_chunk = kSbufBytes / 12;
+  // a batch's film buffer may take 16 GiB (of 180), so that a typical batch
+  // is one chunk with one drain at its end
+  uint64_t const max_chunk = 2 * kSbufBytes / 12;
   uint64_t const chunk = g < max_chunk ? g : max_chunk;
   cudaError_t e = ensure(ctx->jobs, n);
   if (e == cudaSuccess) e = ensure(ctx->job_items, n + 1);

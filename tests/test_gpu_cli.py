@@ -75,7 +75,7 @@ def read_png_rgb(path):
         assert depth == 8
         vals = rows.reshape(h, w, channels)
     if ctype == 3:
-        return plte[vals]
+        return plte[vals.reshape(h, w)]
     if ctype in (0, 4):
         # grey below 8 bits is scaled to the full byte range
         g = vals * (255 // ((1 << depth) - 1)) if depth < 8 else vals[..., 0]
@@ -114,6 +114,17 @@ def test_reference_cli_renders_on_the_gpu(tmp_path):
     ctx.upload(load_nls(nls))
     img = ctx.render(16, 8, 0.8, seed=0)
     assert np.array_equal(raw, Rendering(img).rgb24())
+    # the tone-mapped PNG: the reference's own toneMap (CPU) of this image
+    # (the CLI is built with FMA contraction, the oracle without: bytes
+    # agree to 1)
+    from oracle import refharness
+    tm = np.zeros_like(img)
+    b24 = np.zeros(img.shape, np.uint8)
+    refharness.RefScene(nls).L.ref_tonemap(img.ctypes.data, img.shape[1], img.shape[0], 0.12, tm.ctypes.data,
+                                           b24.ctypes.data)
+    mapped = read_png_rgb(str(bin_dir / "render" / "mixed-16spp-8b-0.80p.png"))
+    assert np.max(np.abs(mapped.astype(int) - b24.astype(int))) <= 1
+    assert len(np.unique(mapped.reshape(-1, 3), axis=0)) > 50
 
 
 def test_reference_cli_fails_loudly_without_a_device(tmp_path):
