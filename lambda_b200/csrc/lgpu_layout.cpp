@@ -518,6 +518,11 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       cents[3 * size_t(i) + r] = 0.5f * (boxes[i].inf[r] + boxes[i].sup[r]);
     }
   }
+  // no objects: an empty instance-BVH box that no ray enters
+  for (int k = 0; k < 3; k++) {
+    L.tlas_bounds[k] = 1e30f;
+    L.tlas_bounds[3 + k] = -1e30f;
+  }
   if (sc.n_objects > 0) {
     RefBvh tl;
     // one object per leaf: objects are culled by the 8-wide box test

@@ -89,6 +89,7 @@ template <bool ANY>
 __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitRec& h, uint32_t skip,
                                            SplitStack& st, TravStats& ts) {
   h.inside = false;
+  if (S.n_objects == 0) return false;
   float const t0 = segment_box_entry(S.tlas_bounds, w, h.z);
   if (t0 == kFltMax) return false;
   st.sp = 0;
@@ -230,6 +231,7 @@ __device__ __forceinline__ void trace_begin(const DevScene& S, TraceState& t, Sp
   t.n_inside = 0;
   t.zs = t.cur_exit = 0.f;
   st.sp = 0;
+  if (S.n_objects == 0) return;  // no instance BVH: every ray misses
   float const t0 = segment_box_entry(S.tlas_bounds, t.w, t.h.z);
   if (t0 != kFltMax) st.push(StackEntry{S.tlas_root, t0});
 }

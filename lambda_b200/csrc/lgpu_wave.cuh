@@ -308,11 +308,11 @@ __device__ __forceinline__ void add_shadow(const WaveState& w, uint32_t s) {
 // per warp once kRefill of them are waiting.
 constexpr int kRefill = 8;
 
-// Occupancy: 6 blocks of 128 per SM (80 registers) for any-hit queries, 5
-// (96 registers, no spills with the row-wise box test and the sorted push)
-// for closest-hit queries.
+// Occupancy (measured best): 7 blocks of 128 per SM (72 registers) for
+// any-hit queries, 5 (96 registers, no spills with the row-wise box test and
+// the sorted push) for closest-hit queries.
 template <bool ANY, int K, class J>
-__global__ void __launch_bounds__(128, ANY ? 6 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
