@@ -69,10 +69,8 @@ def build(force=False, verbose=False, extra_flags=()):
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(BUILD_DIR, src + ".o")
-        # -ffp-contract=off: the host layout precomputes triangle terms that
-        # must round exactly as the device's separate IEEE operations
-        cmds.append([nvcc()] + common + ["-Xcompiler", "-pthread,-ffp-contract=off", "-x", "c++", "-c",
-                                         os.path.join(CSRC, src), "-o", obj])
+        cmds.append([nvcc()] + common + ["-Xcompiler", "-pthread", "-x", "c++", "-c", os.path.join(CSRC, src),
+                                         "-o", obj])
         objs.append(obj)
     procs = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.STDOUT) for c in cmds]
     logs = []

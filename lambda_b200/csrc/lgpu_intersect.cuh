@@ -298,23 +298,26 @@ __device__ __forceinline__ bool push_children(const WideNode& nd, const Ray& r, 
 // intersect::triangle (cg.hpp:1341-1379); mr = l_ray.p ^ l_ray.u.
 __device__ __forceinline__ bool tri_test(const TriSlot& T, const Ray& l, f3 mr, float z,
                                          float& t_out, float& b0, float& b1, float& b2) {
-  const float4* q = reinterpret_cast<const float4*>(T.q);
-  float4 const q0 = q[0], q1 = q[1];
-  f3 const n = mk(q1.x, q1.y, q1.z);
+  f3 const v0 = mk(T.v0[0], T.v0[1], T.v0[2]);
+  f3 const v1 = mk(T.v1[0], T.v1[1], T.v1[2]);
+  f3 const v2 = mk(T.v2[0], T.v2[1], T.v2[2]);
+  f3 const e0 = sub3(v1, v0);
+  f3 const e2 = sub3(v0, v2);
+  f3 const n = cross3(e2, e0);
   float const D = dot3(l.u, n);
   if (fabsf(D) < kEps) return false;
-  float4 const q2 = q[2], q3 = q[3], q4 = q[4], q5 = q[5], q6 = q[6];
-  f3 const e0 = mk(q1.w, q2.x, q2.y), e1 = mk(q2.z, q2.w, q3.x), e2 = mk(q3.y, q3.z, q3.w);
-  f3 const m0 = mk(q4.x, q4.y, q4.z), m1 = mk(q4.w, q5.x, q5.y), m2 = mk(q5.z, q5.w, q6.x);
+  f3 const m0 = cross3(v0, e0);
   float const s0 = ad(dot3(l.u, m0), dot3(e0, mr));
   if (ml(s0, D) < 0.f) return false;
+  f3 const e1 = sub3(v2, v1);
+  f3 const m1 = cross3(v1, e1);
   float const s1 = ad(dot3(l.u, m1), dot3(e1, mr));
   if (ml(s1, D) < 0.f) return false;
+  f3 const m2 = cross3(v2, e2);
   float const s2 = ad(dot3(l.u, m2), dot3(e2, mr));
   if (ml(s2, D) < 0.f) return false;
   if (fabsf(ad(ad(s0, s1), s2)) < kEps) return false;
   float const inv_D = dv(1.f, D);
-  f3 const v0 = mk(q0.x, q0.y, q0.z);
   float const t = ml(dot3(sub3(v0, l.p), n), inv_D);
   if (t < kBias || z < t) return false;
   t_out = t;
@@ -408,7 +411,7 @@ __device__ __forceinline__ bool trimesh_hit(const DevScene& S, uint32_t obj_id, 
       if (tri_test(T, l, mr, h.z, t, b0, b1, b2)) {
         h.z = t;
         h.obj = obj_id;
-        h.face = __float_as_uint(T.q[3]);
+        h.face = __float_as_uint(T.v0[3]);
         h.b0 = b0;
         h.b1 = b1;
         h.b2 = b2;

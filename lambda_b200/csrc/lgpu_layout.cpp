@@ -294,40 +294,6 @@ void parallel_for(size_t n, F fn) {
   for (auto& t : ts) t.join();
 }
 
-// a ^ b in single precision, each product and difference rounded (the
-// device's cross3; this file is compiled without contraction)
-inline void cross_f(const float* a, const float* b, float* out) {
-  float const p0 = a[1] * b[2], p1 = a[2] * b[1];
-  float const p2 = a[2] * b[0], p3 = a[0] * b[2];
-  float const p4 = a[0] * b[1], p5 = a[1] * b[0];
-  out[0] = p0 - p1;
-  out[1] = p2 - p3;
-  out[2] = p4 - p5;
-}
-
-// TriSlot of triangle (a, b, c) with face id f (see lgpu_scene.h)
-void tri_slot(const float* a, const float* b, const float* c, uint32_t f, TriSlot& ts) {
-  float e0[3], e1[3], e2[3], n[3], m0[3], m1[3], m2[3];
-  for (int i = 0; i < 3; i++) {
-    e0[i] = b[i] - a[i];
-    e1[i] = c[i] - b[i];
-    e2[i] = a[i] - c[i];
-  }
-  cross_f(e2, e0, n);
-  cross_f(a, e0, m0);
-  cross_f(b, e1, m1);
-  cross_f(c, e2, m2);
-  float* q = ts.q;
-  q[0] = a[0], q[1] = a[1], q[2] = a[2];
-  std::memcpy(&q[3], &f, 4);
-  q[4] = n[0], q[5] = n[1], q[6] = n[2], q[7] = e0[0];
-  q[8] = e0[1], q[9] = e0[2], q[10] = e1[0], q[11] = e1[1];
-  q[12] = e1[2], q[13] = e2[0], q[14] = e2[1], q[15] = e2[2];
-  q[16] = m0[0], q[17] = m0[1], q[18] = m0[2], q[19] = m1[0];
-  q[20] = m1[1], q[21] = m1[2], q[22] = m2[0], q[23] = m2[1];
-  q[24] = m2[2], q[25] = q[26] = q[27] = 0.f;
-}
-
 bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
 
 }  // namespace
@@ -475,7 +441,18 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       for (size_t s = s0; s < s1; s++) {
         uint32_t const f = m.prim_idxs[s];
         const uint32_t* t = m.F + size_t(f) * m.f_stride;
-        tri_slot(m.V + 3 * size_t(t[0]), m.V + 3 * size_t(t[1]), m.V + 3 * size_t(t[2]), f, tris[s]);
+        TriSlot& ts = tris[s];
+        const float* a = m.V + 3 * size_t(t[0]);
+        const float* b = m.V + 3 * size_t(t[1]);
+        const float* c = m.V + 3 * size_t(t[2]);
+        for (int i = 0; i < 3; i++) {
+          ts.v0[i] = a[i];
+          ts.v1[i] = b[i];
+          ts.v2[i] = c[i];
+        }
+        std::memcpy(&ts.v0[3], &f, 4);
+        ts.v1[3] = 0.f;
+        ts.v2[3] = 0.f;
       }
     });
     parallel_for(m.n_faces, [&](size_t f0, size_t f1) {

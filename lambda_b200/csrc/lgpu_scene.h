@@ -7,8 +7,7 @@
 //   nodes     WideNode[...]             8-wide BVH nodes of every mesh, then
 //                                       the instance-level BVH (TLAS)
 //   tris      TriSlot[...]              leaf triangles in leaf order
-//                                       (v0, n, e0-e2, m0-m2 in 7 float4,
-//                                       face id in the 4th float)
+//                                       (3 x float4, face id in v0.w)
 //   shade     FaceShade[...]            per-face vertex normals + geometric
 //                                       normal, indexed by mesh face_base+face
 //   spectra   float[n_spectra*n_bins]   coefficient spectra
@@ -49,15 +48,11 @@ struct alignas(16) WideNode {
 };
 static_assert(sizeof(WideNode) == 224, "WideNode is 7 sectors of 32 B");
 
-// A leaf triangle with the ray-independent terms of the reference's
-// Plücker test (cg.hpp:1341-1379) computed once on the host, in the same
-// float operations (e0 = v1 - v0, e1 = v2 - v1, e2 = v0 - v2, n = e2 ^ e0,
-// m_i = v_i ^ e_i): 25 floats packed in 7 float4.
 struct alignas(16) TriSlot {
-  float q[28];  // v0.xyz, face id bits | n.xyz, e0.x | e0.yz, e1.xy | e1.z, e2.xyz |
-                // m0.xyz, m1.x | m1.yz, m2.xy | m2.z, 0, 0, 0
+  float v0[4];  // xyz + face id bits in [3]
+  float v1[4];
+  float v2[4];
 };
-static_assert(sizeof(TriSlot) == 112, "TriSlot is 7 float4");
 
 struct FaceShade {
   float n0[3], n1[3], n2[3];

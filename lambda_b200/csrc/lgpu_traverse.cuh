@@ -126,7 +126,7 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
         if (tri_test(T, l, mr, h.z, t, b0, b1, b2)) {
           h.z = t;
           h.obj = cur;
-          h.face = __float_as_uint(T.q[3]);
+          h.face = __float_as_uint(T.v0[3]);
           h.b0 = b0;
           h.b1 = b1;
           h.b2 = b2;
@@ -271,7 +271,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
       if (tri_test(T, t.l, t.mr, h.z, tt, b0, b1, b2)) {
         h.z = tt;
         h.obj = t.cur;
-        h.face = __float_as_uint(T.q[3]);
+        h.face = __float_as_uint(T.v0[3]);
         h.b0 = b0;
         h.b1 = b1;
         h.b2 = b2;
