@@ -235,6 +235,7 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
     pb->beta = c.take<float>(size_t(K) * n);
     pb->acc = c.take<float>(size_t(K) * n);
     pb->gw = adjoint ? c.take<float>(size_t(K) * n) : nullptr;
+    pb->sidx = c.take<uint32_t>(n);
   }
   ws.hit = c.take<float>(9 * n);
   ws.e_acc = c.take<float>(size_t(K) * n);
@@ -242,8 +243,10 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
   ws.e_item = c.take<uint32_t>(n);
   ws.e_job = batch ? c.take<uint32_t>(n) : nullptr;
   ws.sray = c.take<float>(8 * n);
-  ws.s_target = c.take<uint32_t>(n);
+  ws.e_sidx = c.take<uint32_t>(n);
   ws.s_contrib = c.take<float>(size_t(K) * n);
+  ws.s_prev = c.take<float>(size_t(K) * n);
+  ws.s_vis = c.take<uint8_t>(n);
   ws.s_job = batch ? c.take<uint32_t>(n) : nullptr;
   ws.fb_queue = c.take<uint32_t>(n);
   ws.ctl = c.take<uint32_t>(kCtlWords);

@@ -30,6 +30,7 @@ struct PathBuf {
   float* beta;      // K*cap
   float* acc;       // K*cap (path replay: the radiance still to come)
   float* gw;        // K*cap, path replay: dL/d(radiance) per hero wavelength
+  uint32_t* sidx;   // cap: the path's shadow ray of the last iteration, or kNoShadow
 };
 
 // Counters of the wavefront renderer (WaveState::ctl).
@@ -44,7 +45,7 @@ constexpr int kCtlNew = 8;       // plan of the next generate: new paths,
 constexpr int kCtlFirst = 9;     //   their first work item,
 constexpr int kCtlPos = 10;      //   their first queue position
 constexpr int kCtlWords = 16;
-constexpr uint32_t kEndedBit = 0x80000000u;
+constexpr uint32_t kNoShadow = 0xFFFFFFFFu;
 
 // Device buffers of the wavefront renderer; the context owns them.
 struct WaveState {
@@ -61,8 +62,10 @@ struct WaveState {
   uint32_t* e_item;    // cap
   uint32_t* e_job;     // cap (batched renders only)
   float* sray;         // 8*cap shadow rays (ox, oy, oz, dx, dy, dz, tmax, skip)
-  uint32_t* s_target;  // cap: path of each shadow ray (`out` index, or ended index | kEndedBit)
-  float* s_contrib;    // K*cap
+  uint32_t* e_sidx;    // cap: the ended path's last shadow ray, or kNoShadow
+  float* s_contrib;    // K*cap: contributions of this iteration's shadow rays
+  float* s_prev;       // K*cap: those of the last iteration (swapped with s_contrib)
+  uint8_t* s_vis;      // cap: 1 if the shadow ray reached its light
   uint32_t* s_job;     // cap (batched renders only)
   uint32_t* fb_queue;  // cap: `in` indices re-traced in the reference's object order
   uint32_t* ctl;       // kCtlWords counters

@@ -166,7 +166,8 @@ void launch_closest(const J& jobs, const WaveState& w, const WaveGrids& g, bool 
   }
 }
 
-// Swaps the current and next queue after an iteration.
+// Swaps the current and next queue, and the shadow contributions of this
+// and the last iteration, after an iteration.
 inline void swap_queues(WaveState& w) {
   PathBuf const pb = w.in;
   w.in = w.out;
@@ -174,6 +175,9 @@ inline void swap_queues(WaveState& w) {
   uint32_t* const pc = w.n_in;
   w.n_in = w.n_out;
   w.n_out = pc;
+  float* const sc = w.s_contrib;
+  w.s_contrib = w.s_prev;
+  w.s_prev = sc;
 }
 
 // The chunk is done when every work item was started and the queue is

@@ -4,20 +4,21 @@
 // its state at index i of the `in` buffers (field-major, so a warp's access
 // to one field is one coalesced transaction).  Each iteration
 //
-//   wf_finish<K>          ended paths of the last iteration -> XYZ of their
-//                         (sample, pixel) film entry
+//   wf_finish<K>          ended paths of the last iteration (with the light
+//                         sample of their last vertex if its shadow ray got
+//                         through) -> XYZ of their (sample, pixel) film entry
 //   wf_plan               how many new paths fit behind the queue
 //   wf_generate_stream<K> camera ray + hero wavelengths of the new paths,
 //                         appended to the queue
 //   wf_trace_*            closest hit of every queued path
-//   wf_shade<K>           emitters, light sample -> shadow ray, material
-//                         sample -> next ray; a continuing path is written
-//                         to the next position of the `out` queue, an
-//                         ended one to the ended list
+//   wf_shade<K>           adds the last vertex's light sample if its shadow
+//                         ray got through; emitters, light sample -> shadow
+//                         ray, material sample -> next ray; a continuing
+//                         path is written to the next position of the `out`
+//                         queue, an ended one to the ended list
 //   wf_shadow / wf_trace_persistent<true>
-//                         any-hit test of the shadow rays; an unoccluded
-//                         ray adds its radiance to its path (in `out` or in
-//                         the ended list)
+//                         any-hit test of the shadow rays: one visibility
+//                         byte per ray
 //
 // then the host swaps `in` and `out`.  No path keeps a fixed slot, so no
 // access is scattered.  Each path draws its random numbers from its own
@@ -164,6 +165,7 @@ __global__ void __launch_bounds__(256) wf_generate_stream(J jobs, WaveState w, D
     in.hero[p] = hero;
     in.depth[p] = 0;
     in.item[p] = q;
+    in.sidx[p] = kNoShadow;
     if (J::kMulti) in.job[p] = jb;
     if (w.vis) w.vis[q] = 0;
 #pragma unroll
@@ -190,20 +192,22 @@ __global__ void __launch_bounds__(256) wf_finish(J jobs, WaveState w, DevCounter
     float const step = omega / float(K);
     float const prob_l = 1.f / omega;
     float const hero = w.e_hero[e];
+    // the light sample of the path's last vertex, if its shadow ray got through
+    uint32_t const sx_i = w.e_sidx[e];
+    bool const lit = sx_i != kNoShadow && w.s_vis[sx_i];
     float sx = 0.f, sy = 0.f, sz = 0.f;
     bool finite = true;
 #pragma unroll
     for (int k = 0; k < K; k++) {
-      float const val = w.e_acc[k * cap + e] / prob_l;
+      float acc = w.e_acc[k * cap + e];
+      if (lit) acc += w.s_prev[k * cap + sx_i];
+      if (w.ltot) w.ltot[size_t(w.e_item[e]) * K + k] = acc;
+      float const val = acc / prob_l;
       finite = finite && isfinite(val);
       splat_xyz(S, hero_lambda(S, hero, step, k), val, sx, sy, sz);
     }
     nonfinite += finite ? 0u : 1u;
     size_t const o = 3 * size_t(w.e_item[e]);
-    if (w.ltot) {
-#pragma unroll
-      for (int k = 0; k < K; k++) w.ltot[size_t(w.e_item[e]) * K + k] = w.e_acc[k * cap + e];
-    }
     w.sbuf[o] = sx;
     w.sbuf[o + 1] = sy;
     w.sbuf[o + 2] = sz;
@@ -288,17 +292,12 @@ __global__ void __launch_bounds__(128) wf_trace(J jobs, WaveState w, DevCounters
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 
-// Adds an unoccluded shadow ray's radiance to its path: target bit 31 set
-// means the ended list, else the `out` queue.
-template <int K>
-__device__ __forceinline__ void add_shadow(const WaveState& w, uint32_t s) {
-  uint32_t const t = w.s_target[s];
-  float* acc = (t & kEndedBit) ? w.e_acc : w.out.acc;
-  uint32_t const idx = t & ~kEndedBit;
-  uint32_t const cap = w.cap;
-#pragma unroll
-  for (int k = 0; k < K; k++) acc[k * cap + idx] += w.s_contrib[k * cap + s];
-  if (w.vis) w.vis[w.s_item[s]] |= 1ull << w.s_depth[s];
+// Records whether shadow ray s reached its light.  Its radiance is added
+// to the path by the next iteration's shading (or by wf_finish for an ended
+// path), which reads the path's contributions in queue order, coalesced.
+__device__ __forceinline__ void shadow_done(const WaveState& w, uint32_t s, bool unoccluded) {
+  w.s_vis[s] = unoccluded ? 1 : 0;
+  if (unoccluded && w.vis) w.vis[w.s_item[s]] |= 1ull << w.s_depth[s];
 }
 
 // Persistent instance-BVH traversal of the extension rays (ANY = false,
@@ -365,7 +364,7 @@ __global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, 
     if (active && trace_step<ANY>(jobs.scene(jb), t, st, ts)) {
       active = false;
       if (ANY) {
-        if (!t.hit_any) add_shadow<K>(w, idx);
+        shadow_done(w, idx, !t.hit_any);
         continue;
       }
       uint32_t const p = idx;
@@ -447,9 +446,11 @@ __global__ void __launch_bounds__(128) wf_trace_fallback(J jobs, WaveState w, De
 constexpr int kSortGroups = 8;
 
 template <class J>
-__device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveState& w, uint32_t base, uint32_t n) {
+__device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveState& w, uint32_t base, uint32_t n,
+                                                   uint32_t* group = nullptr) {
   __shared__ uint32_t counts[kSortGroups][4];
   __shared__ uint16_t perm[128];
+  __shared__ uint8_t groups[128];
   uint32_t const t = threadIdx.x, lane = t & 31u, wid = t >> 5, nw = blockDim.x >> 5;
   uint32_t const q = base + t;
   uint32_t key = kSortGroups - 1;
@@ -476,8 +477,10 @@ __device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveStat
     for (uint32_t v = 0; v < nw; v++) pos += counts[b][v];
   for (uint32_t v = 0; v < wid; v++) pos += counts[key][v];
   perm[pos] = uint16_t(t);
+  groups[pos] = uint8_t(key);
   __syncthreads();
   uint32_t const r = base + perm[t];
+  if (group) *group = groups[t];
   __syncthreads();  // counts and perm are reused by the block's next chunk
   return r;
 }
@@ -486,7 +489,19 @@ __device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveStat
 // queued path: emitter hit (73-84), light importance sample with the MIS
 // power heuristic (87-113, its visibility left to the shadow kernel),
 // material importance sample with Russian roulette (115-143).
-template <int K, class J>
+// MT < 0: every path; MT = LGPU_MAT_BLINN or LGPU_MAT_THINFILM: only the
+// paths that hit that material (its code alone, the others' branches fold
+// away); MT = LGPU_MAT_LAMBERTIAN: every other path (misses, emitters,
+// Lambertian and unshaded materials).  The three specialised launches
+// together shade every path once.
+template <int MT>
+__device__ __forceinline__ bool shade_group(uint32_t group) {
+  if (MT < 0) return true;
+  if (MT == LGPU_MAT_BLINN || MT == LGPU_MAT_THINFILM) return group == 1u + MT;
+  return group != 1u + LGPU_MAT_BLINN && group != 1u + LGPU_MAT_THINFILM;
+}
+
+template <int K, class J, int MT = -1>
 __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
@@ -494,13 +509,21 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
   PathBuf const& out = w.out;
   enum : int { kEnd = 0, kEmit = 1, kScatter = 2 };
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-    uint32_t const i = material_order(jobs, w, base, n);
-    bool const live = i < n;
+    uint32_t group = 0;
+    uint32_t const i = material_order(jobs, w, base, n, &group);
+    bool const live = i < n && shade_group<MT>(group);
     uint32_t const jb = (J::kMulti && live) ? in.job[i] : 0u;
     const DevScene& S = jobs.scene(jb);
     const RenderArgs& a = jobs.args(jb);
     float const omega = S.lambda_sup - S.lambda_inf;
     float const step = omega / float(K);
+    // the material as this launch sees it: a specialised launch knows its
+    // type at compile time
+    auto material = [&](uint32_t idx) {
+      DevMaterial x = S.mats[idx];
+      if (MT == LGPU_MAT_BLINN || MT == LGPU_MAT_THINFILM) x.type = MT;
+      return x;
+    };
     int kind = kEnd;
     bool cont = false, shadow = false, needs_test = false;
     f3 sp = f3{0.f, 0.f, 0.f}, sd = f3{0.f, 0.f, 1.f};
@@ -532,7 +555,7 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
         f3 const nn = H.front ? H.F.z : neg3(H.F.z);
         mat = H.mat;
         front = H.front;
-        const DevMaterial& m = S.mats[mat];
+        DevMaterial const m = material(mat);
         if (m.type == LGPU_MAT_EMITTER || m.type == LGPU_MAT_DIREMITTER) {
           kind = kEmit;
           if (m.type == LGPU_MAT_DIREMITTER) {
@@ -579,7 +602,11 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
     uint32_t const s_pos = warp_append(w.ctl + kCtlShadow, shadow);
     if (!live) continue;
     float* const acc_dst = cont ? out.acc + o_pos : w.e_acc + e_pos;
-    const DevMaterial& m = S.mats[mat];
+    DevMaterial const m = material(mat);
+    // the light sample of the path's previous vertex, if its shadow ray got
+    // through (recorded by the shadow kernel of the last iteration)
+    uint32_t const prev_s = in.sidx[i];
+    const float* const pend = (prev_s != kNoShadow && w.s_vis[prev_s]) ? w.s_prev + prev_s : nullptr;
     if (kind == kScatter) {
       const lgpu_light& L = S.lights[light];
       for (int k = 0; k < K; k++) {
@@ -590,6 +617,7 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
         float const b = in.beta[k * cap + i];
         float const contrib = b * (rad * coef * lis_scale);
         float acc = in.acc[k * cap + i];
+        if (pend) acc += pend[k * cap];
         if (!needs_test) acc += contrib;
         else if (shadow) w.s_contrib[k * cap + s_pos] = contrib;
         if (cont) out.beta[k * cap + o_pos] = b * (mat_mult_k(S, m, ms, x, l, front) * m_scale);
@@ -598,11 +626,13 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
     } else if (kind == kEmit) {
       for (int k = 0; k < K; k++) {
         float const x = lam_coord(S, hero_lambda(S, hero, step, k));
-        acc_dst[k * cap] = in.acc[k * cap + i] + in.beta[k * cap + i] * (spec_at(S, m.spectrum[0], x) * g_emit);
+        float acc = in.acc[k * cap + i];
+        if (pend) acc += pend[k * cap];
+        acc_dst[k * cap] = acc + in.beta[k * cap + i] * (spec_at(S, m.spectrum[0], x) * g_emit);
       }
     } else {
 #pragma unroll
-      for (int k = 0; k < K; k++) acc_dst[k * cap] = in.acc[k * cap + i];
+      for (int k = 0; k < K; k++) acc_dst[k * cap] = in.acc[k * cap + i] + (pend ? pend[k * cap] : 0.f);
     }
     if (cont) {
       out.ray[0 * cap + o_pos] = np.x;
@@ -615,14 +645,15 @@ __global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCount
       out.hero[o_pos] = hero;
       out.depth[o_pos] = in.depth[i] + 1;
       out.item[o_pos] = in.item[i];
+      out.sidx[o_pos] = shadow ? s_pos : kNoShadow;
       if (J::kMulti) out.job[o_pos] = jb;
     } else {
       w.e_hero[e_pos] = hero;
       w.e_item[e_pos] = in.item[i];
+      w.e_sidx[e_pos] = shadow ? s_pos : kNoShadow;
       if (J::kMulti) w.e_job[e_pos] = jb;
     }
     if (shadow) {
-      w.s_target[s_pos] = cont ? o_pos : (e_pos | kEndedBit);
       if (J::kMulti) w.s_job[s_pos] = jb;
       if (w.vis) {
         w.s_item[s_pos] = in.item[i];
@@ -665,7 +696,7 @@ __global__ void __launch_bounds__(128) wf_shadow(J jobs, WaveState w, DevCounter
     uint32_t const skip = __float_as_uint(w.sray[7 * cap + i]);
     bool const occ = scene_trace<true>(S, r, h, skip, ref_order, st, lstack, ltstack, ts);
     rays++;
-    if (!occ) add_shadow<K>(w, i);
+    shadow_done(w, i, !occ);
   }
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
