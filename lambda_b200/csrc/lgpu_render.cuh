@@ -118,7 +118,7 @@ const WaveOccupancy& wave_occupancy() {
     o.gen = blocks_per_sm(wf_generate_stream<K, J>, 256, 0);
     o.fin = blocks_per_sm(wf_finish<K, J>, 256, 0);
     o.fb = blocks_per_sm(wf_trace_fallback<J>, 128, 0);
-    for (int b = 1; b <= 4; b++) o.shade[b] = blocks_per_sm(wf_shade<K, J>, 32 * b, 0);
+    for (int b = 1; b <= 4; b++) o.shade[b] = blocks_per_sm(wf_shade<K, J, LGPU_MAT_LAMBERTIAN>, 32 * b, 0);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -275,15 +275,20 @@ cudaError_t wave_chunk(const J& jobs, WaveState& w, uint64_t c0, uint32_t total,
     run->begin(2, st);
     // one block per queue chunk, not persistent: a block's warps finish
     // their material-sorted groups at different times, and a persistent
-    // block would hold the fast ones at the next chunk's sort barrier
-    wf_shade<K, J><<<(wi.cap + g.shade_block - 1) / g.shade_block, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
+    // block would hold the fast ones at the next chunk's sort barrier.
+    // Three launches, each with one material type's code (Blinn, thin
+    // film, the rest), so an SM's warps share their instructions.
+    uint32_t const sg = (wi.cap + g.shade_block - 1) / g.shade_block;
+    wf_shade<K, J, LGPU_MAT_LAMBERTIAN><<<sg, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
+    wf_shade<K, J, LGPU_MAT_BLINN><<<sg, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
+    wf_shade<K, J, LGPU_MAT_THINFILM><<<sg, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
     run->end(2, st);
     run->begin(1, st);
     if (linear) wf_shadow<K, J><<<g.shadow, 128, kTraceSmem, st>>>(jobs, wi, c_shadow);
     else wf_trace_persistent<true, K, J><<<g.pshadow, 128, kTraceSmem, st>>>(jobs, wi, c_shadow);
     run->end(1, st);
-    // finish, plan, generate, trace (+ fallback), shade, shadow
-    run->total += linear ? 6 : 7;
+    // finish, plan, generate, trace (+ fallback), shade (3), shadow
+    run->total += linear ? 8 : 9;
   });
   if (e != cudaSuccess) return e;
   wf_finish<K, J><<<g.fin, 256, 0, st>>>(jobs, w, d_cnt);
