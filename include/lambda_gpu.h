@@ -353,6 +353,65 @@ int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,
                        uint32_t flags, lgpu_hit* out);
 
+/* Unit probe of the device's shading functions (the parity probe for
+   materials and lights, as lgpu_trace_closest is for hits).  Each query
+   evaluates one function of the uploaded scene (slot 0) with the render
+   kernels' own device code:
+     LGPU_PROBE_BXDF             BxDFcosθ(λ, materials[index], i, o, n, front)
+                                 (cg.hpp:1088-1102) -> value[k]
+     LGPU_PROBE_PROB_MATERIAL    probForMateriali(λ0, materials[index], hit, i, o, p)
+                                 with the reference's call-site argument order
+                                 (src/renderer.cpp:136-137, cg.hpp:1971-1985) -> prob
+     LGPU_PROBE_SAMPLE_MATERIAL  sample::materiali(λ, materials[index], hit, o, p)
+                                 (cg.hpp:1953-1968) with the uniform draws xi
+                                 -> ok, dir, prob, value[k] = mult
+     LGPU_PROBE_SAMPLE_LIGHT     sample::light(λ, lights[index], hit) (cg.hpp:
+                                 1560-1732) without its shadow ray -> dir,
+                                 prob, value[k] = mult if the light is visible,
+                                 tmax / skip of the shadow ray (tmax < 0: none)
+     LGPU_PROBE_PROB_LIGHT       probForLight(lights[index], ray(p, i))
+                                 (cg.hpp:1735-1747) -> prob
+     LGPU_PROBE_SPECTRUM         spectrum `index` of the scene at λ
+                                 (coefficientλ::operator(), cg.hpp:298-303) -> value[k]
+   The hit is (p, frame F = x, y, z with z the shading normal, front).  xi
+   holds the uniform draws in the order the device consumes them (the draws
+   of f(a(), b()) are a's then b's).  value has hero_k entries. */
+enum {
+  LGPU_PROBE_BXDF = 0,
+  LGPU_PROBE_PROB_MATERIAL = 1,
+  LGPU_PROBE_SAMPLE_MATERIAL = 2,
+  LGPU_PROBE_SAMPLE_LIGHT = 3,
+  LGPU_PROBE_PROB_LIGHT = 4,
+  LGPU_PROBE_SPECTRUM = 5
+};
+
+typedef struct lgpu_probe {
+  uint32_t op;
+  uint32_t index;    /* material, light or spectrum index */
+  float lambda[16];  /* hero wavelengths in nm (the first hero_k are used) */
+  float p[3];        /* hit point */
+  float F[9];        /* shading frame: x, y, z axes */
+  float i[3];        /* incident (light) direction; the ray direction of PROB_LIGHT */
+  float o[3];        /* outgoing (view) direction */
+  float n[3];        /* the normal argument of BXDF */
+  uint32_t front;
+  float sample_p;    /* SAMPLE_P */
+  float xi[4];
+} lgpu_probe;
+
+typedef struct lgpu_probe_result {
+  float value[16];
+  float prob;
+  float dir[3];
+  float tmax;
+  uint32_t skip;
+  uint32_t ok;
+  uint32_t n_xi; /* draws consumed */
+} lgpu_probe_result;
+
+int lgpu_probe_shading(lgpu_ctx* ctx, const lgpu_probe* queries, uint64_t n,
+                       lgpu_probe_result* out);
+
 /* Renderer::toneMap (src/renderer.cpp:149-176) followed by the 8-bit sRGB
    encode of rendering::rgb24 (include/renderer.hpp:20-29).  Either output
    may be NULL.  Host buffers of w*h*3 elements. */

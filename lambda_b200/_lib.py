@@ -7,6 +7,8 @@ does not export the ABI, an ImportError-style RuntimeError is raised.
 import ctypes
 import os
 
+import numpy as np
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblambda_gpu.so")
 
@@ -116,6 +118,17 @@ class Hit(ctypes.Structure):
                 ("gn", ctypes.c_float * 3), ("front", ctypes.c_uint32)]
 
 
+# lgpu_probe_shading (include/lambda_gpu.h): queries and results as numpy
+# records with the C structs' layout (4-byte fields, no padding)
+PROBE_BXDF, PROBE_PROB_MATERIAL, PROBE_SAMPLE_MATERIAL, PROBE_SAMPLE_LIGHT, PROBE_PROB_LIGHT, \
+    PROBE_SPECTRUM = range(6)
+PROBE_DTYPE = np.dtype([("op", "<u4"), ("index", "<u4"), ("lambda", "<f4", 16), ("p", "<f4", 3),
+                        ("F", "<f4", 9), ("i", "<f4", 3), ("o", "<f4", 3), ("n", "<f4", 3),
+                        ("front", "<u4"), ("sample_p", "<f4"), ("xi", "<f4", 4)])
+PROBE_RESULT_DTYPE = np.dtype([("value", "<f4", 16), ("prob", "<f4"), ("dir", "<f4", 3),
+                               ("tmax", "<f4"), ("skip", "<u4"), ("ok", "<u4"), ("n_xi", "<u4")])
+
+
 class Stats(ctypes.Structure):
     _fields_ = [("last_kernel_ms", ctypes.c_double), ("rays", ctypes.c_uint64),
                 ("paths", ctypes.c_uint64), ("device_checks", ctypes.c_uint32),
@@ -152,6 +165,7 @@ SIGNATURES = {
     "lgpu_autotune_batch": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.POINTER(WaveConfig)]),
     "lgpu_trace_closest": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),
+    "lgpu_probe_shading": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp]),
     "lgpu_tonemap": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                     _vp, _vp]),
     "lgpu_get_stats": (ctypes.c_int, [_vp, ctypes.POINTER(Stats)]),

@@ -23,7 +23,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 CU_SOURCES = ["lgpu_api.cu", "lgpu_kernels.cu", "lgpu_render_k4.cu", "lgpu_render_k8.cu",
               "lgpu_render_k16.cu", "lgpu_batch_k4.cu", "lgpu_batch_k8.cu", "lgpu_batch_k16.cu",
               "lgpu_adjoint_k4.cu", "lgpu_adjoint_k8.cu", "lgpu_adjoint_k16.cu",
-              "lgpu_noalloc.cu"]
+              "lgpu_noalloc.cu", "lgpu_probe.cu"]
 CPP_SOURCES = ["lgpu_layout.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -59,7 +59,13 @@ def build(force=False, verbose=False, extra_flags=()):
                 return OUT
     os.makedirs(BUILD_DIR, exist_ok=True)
     inc = ["-I" + os.path.join(REPO, "include"), "-I" + CSRC]
-    common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo"] + inc
+    # -fmad=false: no multiply-add contraction, so every float operation
+    # rounds as written.  Kernels instantiated for different job policies and
+    # material specialisations then compute bit-identical paths (a batched
+    # job equals its plain render), and the shading arithmetic matches the
+    # reference's operation for operation except in the transcendental
+    # functions.  Traversal spells out its roundings (__fadd_rn etc.) anyway.
+    common = ["-O3", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-lineinfo"] + inc
     objs = []
     cmds = []
     for src in CU_SOURCES:

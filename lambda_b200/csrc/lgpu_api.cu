@@ -82,6 +82,8 @@ struct lgpu_ctx {
   uint32_t* h_ctl = nullptr;  // pinned
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
+  DevArray<lgpu_probe> probes;
+  DevArray<lgpu_probe_result> probe_out;
   DevArray<double> partials;
   DevArray<float> tm_in, tm_out;
   DevArray<uint8_t> tm_24;
@@ -641,6 +643,8 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   ctx->rays.release();
   ctx->hits.release();
+  ctx->probes.release();
+  ctx->probe_out.release();
   ctx->partials.release();
   ctx->tm_in.release();
   ctx->tm_out.release();
@@ -964,6 +968,43 @@ int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t fl
     e = cudaMemcpyAsync(out, ctx->hits.ptr, n * sizeof(lgpu_hit), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "trace");
   return collect(ctx, "trace");
+}
+
+int lgpu_probe_shading(lgpu_ctx* ctx, const lgpu_probe* queries, uint64_t n, lgpu_probe_result* out) {
+  if (!ctx || (n && (!queries || !out))) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  if (int r = bind_device(ctx)) return r;
+  if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
+  if (n == 0) return LGPU_OK;
+  const DevScene& S = ctx->S;
+  uint64_t const n_spectra = S.n_bins ? ctx->slots[0].spectra.n / S.n_bins : 0;
+  for (uint64_t q = 0; q < n; q++) {
+    lgpu_probe const& Q = queries[q];
+    uint64_t bound = 0;
+    switch (Q.op) {
+      case LGPU_PROBE_BXDF:
+      case LGPU_PROBE_PROB_MATERIAL:
+      case LGPU_PROBE_SAMPLE_MATERIAL: bound = S.n_materials; break;
+      case LGPU_PROBE_SAMPLE_LIGHT:
+      case LGPU_PROBE_PROB_LIGHT: bound = S.n_lights; break;
+      case LGPU_PROBE_SPECTRUM: bound = n_spectra; break;
+      default:
+        return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "probe " + std::to_string(q) + ": unknown op");
+    }
+    if (Q.index >= bound)
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "probe " + std::to_string(q) + ": index out of range");
+  }
+  cudaError_t e = ensure(ctx->probes, n);
+  if (e == cudaSuccess) e = ensure(ctx->probe_out, n);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "probe buffers");
+  cudaStream_t const st = ctx->stream;
+  e = cudaMemcpyAsync(ctx->probes.ptr, queries, n * sizeof(lgpu_probe), cudaMemcpyHostToDevice, st);
+  ctx->stats.launches = 1;
+  if (e == cudaSuccess) e = launch_probe(S, ctx->probes.ptr, n, ctx->probe_out.ptr, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, ctx->probe_out.ptr, n * sizeof(lgpu_probe_result), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "probe");
+  return LGPU_OK;
 }
 
 int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h, float y_mid,

@@ -93,6 +93,10 @@ struct RenderArgs {
   uint32_t stream_tag;   // high bits of the RNG stream id (job id)
 };
 
+// lgpu_probe_shading: one thread per query (lgpu_probe.cu)
+cudaError_t launch_probe(const DevScene& S, const lgpu_probe* d_q, uint64_t n, lgpu_probe_result* d_out,
+                         cudaStream_t st);
+
 cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
                          lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st);
 

@@ -141,6 +141,19 @@ __device__ __forceinline__ float schlick_F0(float n) {
   return (n * n - 2.f * n + 1.f) / (n * n + 2.f * n + 1.f);
 }
 
+// Uniform draws given explicitly (the shading unit probe): the sampling
+// functions below take either a PCG state (uint64_t) or this.
+struct XiDraws {
+  const float* xi;
+  uint32_t n, used;
+};
+using ::lgpu_flt;
+__device__ __forceinline__ float lgpu_flt(XiDraws* r) {
+  float const x = r->used < r->n ? r->xi[r->used] : 0.f;
+  r->used++;
+  return x;
+}
+
 // ---- lights -----------------------------------------------------------------
 
 struct LightSample {
@@ -165,8 +178,9 @@ __device__ __forceinline__ f3 col3(const float* M16, int c) {
 // λ-independent factor of mult assuming the light is visible; tmax and skip
 // describe the shadow ray the reference traces (for sphere lights up to the
 // light's centre, cg.hpp:1696); tmax < 0 means no shadow ray (ambient).
+template <class R>
 __device__ __forceinline__ LightSample sample_light_unoccluded(const DevScene& S, const lgpu_light& L,
-                                                               const HitInfo& H, uint64_t& rng,
+                                                               const HitInfo& H, R& rng,
                                                                float& tmax, uint32_t& skip) {
   LightSample ls;
   ls.scale = 0.f;
@@ -402,8 +416,9 @@ struct MatSample {
   float lnhn;    // log of the |cosine| raised to α in c (for d/dα)
 };
 
+template <class R>
 __device__ __forceinline__ MatSample sample_material(const DevScene& S, const DevMaterial& m, float x0,
-                                                     const HitInfo& H, f3 o, float p, uint64_t& rng) {
+                                                     const HitInfo& H, f3 o, float p, R& rng) {
   MatSample ms;
   ms.ok = false;
   ms.prob = 0.f;

@@ -201,6 +201,15 @@ class Context:
                                                      ctypes.addressof(out)), "trace")
         return hits_to_numpy(out, rays.shape[0])
 
+    def probe(self, queries):
+        """Runs lgpu_probe_shading on a record array of _lib.PROBE_DTYPE;
+        returns a record array of _lib.PROBE_RESULT_DTYPE."""
+        q = np.ascontiguousarray(queries, L.PROBE_DTYPE)
+        out = np.zeros(q.shape[0], L.PROBE_RESULT_DTYPE)
+        L.check(self.h, self._lib.lgpu_probe_shading(self.h, q.ctypes.data, q.shape[0], out.ctypes.data),
+                "probe")
+        return out
+
     def tonemap(self, linrgb, y_mid=0.12):
         img = np.ascontiguousarray(linrgb, np.float32)
         h, w = img.shape[:2]

@@ -38,6 +38,8 @@ def test_struct_sizes_match_c():
     assert ctypes.sizeof(L.RenderParams) == 32
     assert ctypes.sizeof(L.Hit) == 56
     assert ctypes.sizeof(L.Job) == 64
+    assert L.PROBE_DTYPE.itemsize == 180
+    assert L.PROBE_RESULT_DTYPE.itemsize == 96
 
 
 def test_errors_without_arguments():

@@ -3,8 +3,8 @@ the device's own random stream.
 
 With ORACLE_RNG_PCG the oracle draws the same numbers in the same order as
 the render kernel, so both trace the same paths.  They differ only in the
-rounding of shading arithmetic (the device contracts to FMA and uses CUDA's
-sinf/cosf/powf; the oracle uses libm without contraction) and in the film
+rounding of transcendental functions (the device uses CUDA's sincosf/cosf/
+powf, the oracle libm; neither contracts multiply-adds) and in the film
 (the device accumulates XYZ directly, the oracle 80-bin spectra).  Rounding
 can occasionally flip a later branch of a path, so the test asks for:
   * image means equal to 1e-3 relative per channel,
