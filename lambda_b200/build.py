@@ -37,7 +37,8 @@ def nvcc():
 
 def _digest(extra_flags):
     h = hashlib.sha256()
-    names = sorted(os.listdir(CSRC)) + ["../../include/lambda_gpu.h"]
+    # the sources, the ABI header and this file (its compiler flags)
+    names = sorted(os.listdir(CSRC)) + ["../../include/lambda_gpu.h", "../build.py"]
     for n in names:
         p = os.path.normpath(os.path.join(CSRC, n))
         if os.path.isfile(p):
