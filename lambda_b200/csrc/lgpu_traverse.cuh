@@ -20,7 +20,7 @@
 
 namespace lgpu {
 
-constexpr int kSmemStack = 24;
+constexpr int kSmemStack = 16;
 constexpr int kLocalStack = kStackCap + kTlasStackCap + 4 - kSmemStack;
 constexpr uint32_t kMarker = 0xFFFFFFFEu;
 
