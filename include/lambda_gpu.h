@@ -240,6 +240,10 @@ typedef struct lgpu_stats {
   uint64_t kernel_node_tests[3];
   uint64_t kernel_tri_tests[3];
   uint64_t kernel_inst_tests[3];
+  /* extension rays of the last render whose closest hit depends on the
+     reference's object order (more than one mesh whose bounds contain the
+     ray origin), re-traced with its linear object loop */
+  uint64_t order_rays;
 } lgpu_stats;
 
 /* Context.  `device` is a CUDA ordinal. */

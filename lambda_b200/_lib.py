@@ -138,7 +138,7 @@ class Stats(ctypes.Structure):
                 ("upload_bytes", ctypes.c_uint64), ("kernel_ms", ctypes.c_double * 3),
                 ("kernel_launches", ctypes.c_uint64 * 3), ("kernel_rays", ctypes.c_uint64 * 3),
                 ("kernel_node_tests", ctypes.c_uint64 * 3), ("kernel_tri_tests", ctypes.c_uint64 * 3),
-                ("kernel_inst_tests", ctypes.c_uint64 * 3)]
+                ("kernel_inst_tests", ctypes.c_uint64 * 3), ("order_rays", ctypes.c_uint64)]
 
 FLAG_KERNEL_TIMING = 0x4
 KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2

@@ -182,6 +182,7 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
     c.insts += r[k].insts;
     c.flags |= r[k].flags;
     c.nonfinite += r[k].nonfinite;
+    c.ordered += r[k].ordered;
   }
   ctx->stats.rays = c.rays;
   ctx->stats.paths = c.paths;
@@ -190,6 +191,7 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
   ctx->stats.tri_tests = c.tris;
   ctx->stats.inst_tests = c.insts;
   ctx->stats.nonfinite_paths = c.nonfinite;
+  ctx->stats.order_rays = c.ordered;
   ctx->stats.launches = uint32_t(ctx->launch.total);
   for (int k = 0; k < 3; k++) {
     ctx->stats.kernel_ms[k] = timed ? ctx->launch.ms[k] : 0.0;

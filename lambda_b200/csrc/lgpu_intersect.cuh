@@ -453,6 +453,24 @@ __device__ __forceinline__ bool object_hit(const DevScene& S, uint32_t i, const 
   return true;
 }
 
+// Whether object i can be hit by the ray at any distance: object_hit with
+// an unbounded distance.  Every test object_hit makes only gets stricter as
+// the distance bound shrinks, so an object that fails here fails in
+// object_hit whatever hits came before it.
+__device__ __forceinline__ bool object_may_hit(const DevScene& S, uint32_t i, const Ray& w) {
+  const DevObject& ob = S.objects[i];
+  Ray const l = to_local(ob, w);
+  if (ob.type == LGPU_OBJ_TRIMESH) {
+    bool inside;
+    float ex;
+    return aabb_scalar(S.meshes[ob.mesh].bounds, l, kFltMax, inside, ex) != kFltMax;
+  }
+  float t;
+  if (ob.type == LGPU_OBJ_SPHERE) return sphere_test(l, kFltMax, t);
+  f3 x;
+  return plane_test(l, kFltMax, t, x);
+}
+
 // intersect::scene (cg.hpp:1469-1489).  `skip` is an object index to ignore.
 //
 // With reference_order the objects are tested in index order like the

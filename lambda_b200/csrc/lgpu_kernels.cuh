@@ -16,6 +16,7 @@ struct DevCounters {
   unsigned long long insts;  // object tests
   unsigned int flags;        // bit 0: traversal stack overflow
   unsigned int nonfinite;    // paths whose radiance was NaN or infinite
+  unsigned long long ordered; // rays re-traced in the reference's object order
 };
 
 // Path state of one queue of the wavefront renderer (lgpu_wave.cuh): path

@@ -414,21 +414,41 @@ __global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, 
 }
 
 // Extension rays whose closest hit depends on the reference's object order
-// (see scene_hit): the linear object loop.
+// (see scene_hit): the linear object loop, one warp per ray.  The lanes
+// first test 32 objects at a time with an unbounded distance (the objects
+// the ray cannot hit at all drop out); lane 0 then runs the reference's
+// loop over the remaining ones in index order.  A launch has few such rays
+// (about ten), so its time is the latency of one ray's loop, which the
+// filter shortens from every object to the handful the ray can reach.
 template <class J>
 __global__ void __launch_bounds__(128) wf_trace_fallback(J jobs, WaveState w, DevCounters* cnt) {
   StackEntry lstack[kStackCap];
-  StackEntry ltstack[kTlasStackCap];
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t const n = w.ctl[kCtlFallback];
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  uint32_t const lane = threadIdx.x & 31u;
+  uint32_t const nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += nwarps) {
     uint32_t const p = w.fb_queue[i];
     const DevScene& S = jobs.scene(J::kMulti ? w.in.job[p] : 0u);
     Ray const r = load_ray(w.in.ray, w.cap, p);
     HitRec h;
     clear_hit(h, kFltMax);
-    scene_hit<false>(S, r, h, UINT32_MAX, true, lstack, ltstack, ts);
-    store_hit(w, p, h);
+    h.inside = false;
+    for (uint32_t base = 0; base < S.n_objects; base += 32) {
+      uint32_t const o = base + lane;
+      unsigned m = __ballot_sync(0xFFFFFFFFu, o < S.n_objects && object_may_hit(S, o, r));
+      if (lane == 0)
+        while (m) {
+          uint32_t const b = uint32_t(__ffs(m) - 1);
+          m &= m - 1u;
+          object_hit<false>(S, base + b, r, h, lstack, ts, kRefOrder);
+        }
+      __syncwarp();
+    }
+    if (lane == 0) {
+      store_hit(w, p, h);
+      atomicAdd(&cnt->ordered, 1ull);
+    }
   }
   flush_counters(cnt, 0u, 0u, ts, 0u);
 }

@@ -226,7 +226,7 @@ class Context:
                 "device_checks": s.device_checks, "max_stack": s.max_stack,
                 "nonfinite_paths": s.nonfinite_paths, "node_tests": s.node_tests,
                 "tri_tests": s.tri_tests, "inst_tests": s.inst_tests,
-                "upload_bytes": s.upload_bytes, "launches": s.launches,
+                "upload_bytes": s.upload_bytes, "launches": s.launches, "order_rays": s.order_rays,
                 "kernels": [{"ms": s.kernel_ms[k], "launches": s.kernel_launches[k],
                              "rays": s.kernel_rays[k], "node_tests": s.kernel_node_tests[k],
                              "tri_tests": s.kernel_tri_tests[k],
