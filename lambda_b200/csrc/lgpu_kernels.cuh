@@ -104,7 +104,7 @@ cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uin
 // Launch shape of the wavefront, chosen by the autotuner
 // (lgpu_autotune_batch) or set by the caller (lgpu_set_wave_config).
 struct WaveConfig {
-  uint32_t queue_cap = 1u << 21;  // paths in flight
+  uint32_t queue_cap = 1u << 24;  // paths in flight
   uint32_t shade_block = 128;     // threads per block of the shading kernel (32, 64 or 128)
   uint32_t trace_per_sm = 0;      // persistent trace blocks per SM (0: the occupancy limit)
   uint32_t graphs = 1;            // 1: bounce stages replayed from a captured CUDA graph

@@ -255,7 +255,10 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   if (e.t > h.z) return st.sp == 0;
   if (!(e.ref & kLeafBit)) {
     ts.nodes++;
-    if (!push_children_split<true>(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !any)) {
+    // children near to far, except in the shadow kernel: its answer does not
+    // depend on the order, and sorting costs it more than it saves.  (The
+    // closest-hit kernel's own any-hit queries are faster sorted.)
+    if (!push_children_split<true>(S.nodes[e.ref], t.in_mesh ? t.l : t.w, h.z, st, !ANY)) {
       ts.flags |= 1u;
       return true;
     }
