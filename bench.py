@@ -552,6 +552,8 @@ def run_device(args, w):
     fs = flatten(sc)
     ctx = Context(local)
     ctx.upload(fs)
+    if args.queue_cap:
+        ctx.set_wave_config(queue_cap=args.queue_cap)
     W, H = ctx.size
     spp, B, p = w["spp"], w["bounces"], w["p"]
     paths_per_step = W * H * spp
@@ -660,6 +662,8 @@ def main():
     ap.add_argument("--small", action="store_true", help="reduced frame (profiling)")
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--width", type=int, default=None, help="frame width (profiling)")
+    ap.add_argument("--queue-cap", type=int, default=0,
+                    help="paths in flight (profiling a launch of a given size; default: the library's)")
     ap.add_argument("--no-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost and FD check")

@@ -331,10 +331,10 @@ int lgpu_adjoint_device(lgpu_ctx* ctx, const lgpu_render_params* params, const f
 
 /* Launch shape of the wavefront renderer (no counterpart in the reference,
    which renders on CPU threads).  Defaults: queue_cap 2^24, shade_block
-   128, trace_per_sm 0, graphs 1, mega_items 0. */
+   256, trace_per_sm 0, graphs 1, mega_items 0. */
 typedef struct lgpu_wave_config {
   uint32_t queue_cap;    /* paths in flight */
-  uint32_t shade_block;  /* threads per block of the shading kernel: 32, 64, 96 or 128 */
+  uint32_t shade_block;  /* threads per block of the shading kernel: a multiple of 32 up to 256 */
   uint32_t trace_per_sm; /* resident blocks per SM of the persistent trace kernels (0: occupancy limit) */
   uint32_t graphs;       /* 1: the bounce stages are captured once per chunk as a CUDA graph and replayed */
   uint64_t mega_items;   /* batched renders: jobs with fewer work items (pixels x spp) are rendered by

@@ -865,8 +865,8 @@ int lgpu_set_wave_config(lgpu_ctx* ctx, const lgpu_wave_config* c) {
   if (!ctx || !c) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (c->queue_cap < 1024 || c->queue_cap > (1u << 24))
     return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "queue_cap must be in [1024, 2^24]");
-  if (c->shade_block < 32 || c->shade_block > 128 || c->shade_block % 32)
-    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "shade_block must be 32, 64, 96 or 128");
+  if (c->shade_block < 32 || c->shade_block > kMaxShadeBlock || c->shade_block % 32)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "shade_block must be a multiple of 32 up to 256");
   ctx->cfg.queue_cap = c->queue_cap;
   ctx->cfg.shade_block = c->shade_block;
   ctx->cfg.trace_per_sm = c->trace_per_sm;
@@ -939,7 +939,7 @@ int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_
   };
   int rc = try_dim([](WaveConfig& c, uint64_t v) { c.queue_cap = uint32_t(v); },
                    {1u << 20, 1u << 22, 1u << 23, 1u << 24});
-  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.shade_block = uint32_t(v); }, {64, 96, 128});
+  if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.shade_block = uint32_t(v); }, {64, 128, 256});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.trace_per_sm = uint32_t(v); }, {0, 4, 5});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.graphs = uint32_t(v); }, {0, 1});
   if (!rc) rc = try_dim([](WaveConfig& c, uint64_t v) { c.mega_items = v; }, {0, 1u << 14, 1u << 16});

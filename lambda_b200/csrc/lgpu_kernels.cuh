@@ -103,9 +103,14 @@ cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uin
 
 // Launch shape of the wavefront, chosen by the autotuner
 // (lgpu_autotune_batch) or set by the caller (lgpu_set_wave_config).
+// Largest block of the shading kernels, whose queue entries a block sorts
+// by material together: 256 fills a warp with one material more often than
+// 128 (shading -6 %; 512 is no faster)
+constexpr uint32_t kMaxShadeBlock = 256;
+
 struct WaveConfig {
   uint32_t queue_cap = 1u << 24;  // paths in flight
-  uint32_t shade_block = 128;     // threads per block of the shading kernel (32, 64 or 128)
+  uint32_t shade_block = 256;     // threads per block of the shading kernel (multiple of 32, <= 256)
   uint32_t trace_per_sm = 0;      // persistent trace blocks per SM (0: the occupancy limit)
   uint32_t graphs = 1;            // 1: bounce stages replayed from a captured CUDA graph
   uint64_t mega_items = 0;        // batches: jobs with fewer work items run the megakernel

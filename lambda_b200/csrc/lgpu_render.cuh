@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(128) render_kernel(DevScene S, RenderArgs a, f
 struct WaveOccupancy {
   uint32_t sms = 0;
   uint32_t trace, shadow, ptrace, pshadow, gen, fin, fb;
-  uint32_t shade[5];  // 32, 64, 96, 128 threads per block (index block / 32)
+  uint32_t shade[kMaxShadeBlock / 32 + 1];  // 32, 64, ... threads per block (index block / 32)
 };
 constexpr size_t kTraceSmem = size_t(kSmemStack) * 128 * sizeof(StackEntry);
 
@@ -118,7 +118,8 @@ const WaveOccupancy& wave_occupancy() {
     o.gen = blocks_per_sm(wf_generate_stream<K, J>, 256, 0);
     o.fin = blocks_per_sm(wf_finish<K, J>, 256, 0);
     o.fb = blocks_per_sm(wf_trace_fallback<J>, 128, 0);
-    for (int b = 1; b <= 4; b++) o.shade[b] = blocks_per_sm(wf_shade<K, J, LGPU_MAT_LAMBERTIAN>, 32 * b, 0);
+    for (uint32_t b = 1; b <= kMaxShadeBlock / 32; b++)
+      o.shade[b] = blocks_per_sm(wf_shade<K, J, LGPU_MAT_LAMBERTIAN>, 32 * b, 0);
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -136,7 +137,7 @@ struct WaveGrids {
 template <int K, class J>
 WaveGrids wave_grids(const WaveConfig& cfg) {
   const WaveOccupancy& o = wave_occupancy<K, J>();
-  uint32_t const sb = (cfg.shade_block >= 32 && cfg.shade_block <= 128 && cfg.shade_block % 32 == 0)
+  uint32_t const sb = (cfg.shade_block >= 32 && cfg.shade_block <= kMaxShadeBlock && cfg.shade_block % 32 == 0)
                           ? cfg.shade_block
                           : 128;
   auto cap = [&](uint32_t per_sm) { return cfg.trace_per_sm && cfg.trace_per_sm < per_sm ? cfg.trace_per_sm : per_sm; };

@@ -468,9 +468,9 @@ constexpr int kSortGroups = 8;
 template <class J>
 __device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveState& w, uint32_t base, uint32_t n,
                                                    uint32_t* group = nullptr) {
-  __shared__ uint32_t counts[kSortGroups][4];
-  __shared__ uint16_t perm[128];
-  __shared__ uint8_t groups[128];
+  __shared__ uint32_t counts[kSortGroups][kMaxShadeBlock / 32];
+  __shared__ uint16_t perm[kMaxShadeBlock];
+  __shared__ uint8_t groups[kMaxShadeBlock];
   uint32_t const t = threadIdx.x, lane = t & 31u, wid = t >> 5, nw = blockDim.x >> 5;
   uint32_t const q = base + t;
   uint32_t key = kSortGroups - 1;
@@ -522,7 +522,7 @@ __device__ __forceinline__ bool shade_group(uint32_t group) {
 }
 
 template <int K, class J, int MT = -1>
-__global__ void __launch_bounds__(128, 8) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(kMaxShadeBlock, 4) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
   PathBuf const& in = w.in;

@@ -99,7 +99,8 @@ def test_image_independent_of_launch_shape(scenes):
     plain = Context()
     plain.upload(scenes[1])
     p_ref = plain.render(JOBS[1]["spp"], JOBS[1]["max_scatterings"], JOBS[1]["sample_p"], seed=JOBS[1]["seed"])
-    for shape in (dict(queue_cap=4096), dict(shade_block=64), dict(trace_per_sm=3), dict(graphs=0),
+    for shape in (dict(queue_cap=4096), dict(shade_block=64), dict(shade_block=128), dict(trace_per_sm=3),
+                  dict(graphs=0),
                   dict(queue_cap=1 << 22, shade_block=96, graphs=1)):
         ctx.set_wave_config(**shape)
         got = ctx.render_batch(JOBS[:4])
