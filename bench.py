@@ -499,7 +499,7 @@ def cpu_reference_sample(nls, w, budget_s, fast=True, keep=None):
 
 
 def run_reference(args, w):
-    rank = int(os.environ.get("RANK", "0"))
+    rank = rank_env()[1]
     if rank != 0:
         return 0
     from oracle import refharness
@@ -528,15 +528,36 @@ def run_reference(args, w):
     return 0
 
 
+def rank_env():
+    """(world size, rank, local rank) as torch.distributed.run sets them."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(x, dist, device):
+    """The largest x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(paths_per_step, steps, world, total_ms):
+    """Whole-job Mpaths/s: every rank renders its own frame of paths_per_step
+    paths each step (replicas, weak scaling), and the job takes as long as
+    its slowest rank (total_ms, the max over ranks)."""
+    return world * paths_per_step * steps / (total_ms / 1e3) / 1e6
+
+
 def run_device(args, w):
     import torch
 
     from lambda_b200.renderer import Context
     from lambda_b200.scene import flatten, load_nls
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local = rank_env()
     dist = None
     if world > 1:
         import datetime
@@ -590,12 +611,8 @@ def run_device(args, w):
         dist.barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
-    total_ms = sum(step_ms)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * paths_per_step * args.steps / (total_ms / 1e3) / 1e6
+    total_ms = max_over_ranks(sum(step_ms), dist, "cuda")
+    value = job_throughput(paths_per_step, args.steps, world, total_ms)
 
     # end to end through the C ABI with host buffers
     import numpy as np
@@ -608,13 +625,9 @@ def run_device(args, w):
     for k in range(e2e_steps):
         ctx.upload(fs)
         ctx.render(spp, B, p, seed=k, out=host)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
     h2d = ctx.stats()["upload_bytes"]
-    e2e = {"value": world * paths_per_step * e2e_steps / e2e_s / 1e6, "unit": UNIT,
+    e2e = {"value": job_throughput(paths_per_step, e2e_steps, world, e2e_s * 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(W * H * 3 * 4),
            "note": "lgpu_upload_scene (host layout + copies) + lgpu_render (kernel + image "
                    "readback) per step"}
