@@ -459,6 +459,17 @@ int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
                    uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
                    uint32_t* prim_idxs, uint32_t* n_prim_idxs);
 
+/* lgpu_build_bvh on the context's GPU (bvh::build, cg.hpp:632-749, one
+   tree level per step): the same arguments, host arrays in and out, and a
+   bit-identical result.  For hosts that load large meshes without the
+   reference's trimeshdata, so that building their trees does not cost a
+   serial host pass per mesh. */
+int lgpu_build_bvh_device(lgpu_ctx* ctx, const float* V, uint32_t n_positions,
+                          const uint32_t* F, uint32_t f_stride, uint32_t n_faces,
+                          uint32_t* nodes, uint32_t* n_nodes, float* bbs,
+                          uint32_t* n_bbs, uint32_t* prim_idxs,
+                          uint32_t* n_prim_idxs);
+
 #ifdef __cplusplus
 }
 #endif

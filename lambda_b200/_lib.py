@@ -173,6 +173,8 @@ SIGNATURES = {
                                             _vp, _vp, _vp]),
     "lgpu_build_bvh": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
                                       _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
+    "lgpu_build_bvh_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
+                                             _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
 }
 
 _lib = None

@@ -1044,6 +1044,34 @@ int lgpu_get_stats(const lgpu_ctx* ctx, lgpu_stats* out) {
   return LGPU_OK;
 }
 
+int lgpu_build_bvh_device(lgpu_ctx* ctx, const float* V, uint32_t n_positions, const uint32_t* F,
+                          uint32_t f_stride, uint32_t n_faces, uint32_t* nodes, uint32_t* n_nodes, float* bbs,
+                          uint32_t* n_bbs, uint32_t* prim_idxs, uint32_t* n_prim_idxs) {
+  if (!ctx) return LGPU_ERR_INVALID_ARGUMENT;
+  if (!V || !F || f_stride < 3 || n_faces == 0 || !n_nodes || !n_bbs || !n_prim_idxs)
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument, f_stride < 3 or no faces");
+  for (uint32_t f = 0; f < n_faces; f++)
+    for (int k = 0; k < 3; k++)
+      if (F[size_t(f) * f_stride + k] >= n_positions)
+        return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "face " + std::to_string(f) + ": vertex index out of range");
+  if (int r = bind_device(ctx)) return r;
+  RefBvh B;
+  cudaError_t e;
+  try {
+    e = build_bvh_device(V, n_positions, F, f_stride, n_faces, B, ctx->stream);
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, LGPU_ERR_OUT_OF_MEMORY, "host memory for the BVH");
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "device BVH build");
+  *n_nodes = B.n_nodes;
+  *n_bbs = uint32_t(B.bbs.size() / 48);
+  *n_prim_idxs = uint32_t(B.prim_idxs.size());
+  if (nodes) std::memcpy(nodes, B.nodes.data(), B.nodes.size() * sizeof(uint32_t));
+  if (bbs) std::memcpy(bbs, B.bbs.data(), B.bbs.size() * sizeof(float));
+  if (prim_idxs) std::memcpy(prim_idxs, B.prim_idxs.data(), B.prim_idxs.size() * sizeof(uint32_t));
+  return LGPU_OK;
+}
+
 int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F, uint32_t f_stride,
                    uint32_t n_faces, uint32_t* nodes, uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
                    uint32_t* prim_idxs, uint32_t* n_prim_idxs) {

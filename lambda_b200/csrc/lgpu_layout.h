@@ -33,6 +33,17 @@ void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
 void triangle_prims(const float* V, const uint32_t* F, uint32_t f_stride, uint32_t n_faces,
                     std::vector<PrimBox>& boxes, std::vector<float>& centroids);
 
+}  // namespace lgpu
+
+#include <cuda_runtime_api.h>
+
+namespace lgpu {
+
+// build_ref_bvh for a triangle mesh, on the device (lgpu_bvh_build.cu):
+// host arrays in, the same tree out.  Face indices must be valid.
+cudaError_t build_bvh_device(const float* V, uint32_t n_positions, const uint32_t* F, uint32_t f_stride,
+                             uint32_t n_faces, RefBvh& out, cudaStream_t st);
+
 struct HostLayout {
   std::vector<DevObject> objects;
   std::vector<DevMesh> meshes;

@@ -201,6 +201,28 @@ class Context:
                                                      ctypes.addressof(out)), "trace")
         return hits_to_numpy(out, rays.shape[0])
 
+    def build_bvh(self, V, F, device=True):
+        """bvh::build of a triangle mesh (V: positions (n, 3) with the
+        loader's dummy at 0, F: (n_faces, k >= 3) vertex indices first) in
+        the reference's layout, on this context's GPU (device=True) or with
+        the host restatement.  Returns (nodes, bbs, prim_idxs)."""
+        V = np.ascontiguousarray(V, np.float32).reshape(-1, 3)
+        F = np.ascontiguousarray(F, np.uint32)
+        nf, stride = F.shape
+        nodes = np.zeros(4 * nf + 4, np.uint32)
+        bbs = np.zeros(96 * nf + 96, np.float32)
+        prims = np.zeros(nf + 1, np.uint32)
+        nn, nb, npi = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        args = (V.ctypes.data, V.shape[0], F.ctypes.data, stride, nf, nodes.ctypes.data, ctypes.byref(nn),
+                bbs.ctypes.data, ctypes.byref(nb), prims.ctypes.data, ctypes.byref(npi))
+        if device:
+            L.check(self.h, self._lib.lgpu_build_bvh_device(self.h, *args), "build_bvh_device")
+        else:
+            rc = self._lib.lgpu_build_bvh(*args)
+            if rc != 0:
+                raise L.LgpuError(rc, "lgpu_build_bvh failed")
+        return nodes[:2 * nn.value].copy(), bbs[:48 * nb.value].copy(), prims[:npi.value].copy()
+
     def probe(self, queries):
         """Runs lgpu_probe_shading on a record array of _lib.PROBE_DTYPE;
         returns a record array of _lib.PROBE_RESULT_DTYPE."""
