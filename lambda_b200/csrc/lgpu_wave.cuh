@@ -301,11 +301,11 @@ __device__ __forceinline__ void shadow_done(const WaveState& w, uint32_t s, bool
 }
 
 // Persistent instance-BVH traversal of the extension rays (ANY = false,
-// the `in` queue, hit records out) or the shadow rays (ANY = true,
-// unoccluded contributions added to their paths).  A lane that finishes its
-// ray takes the next one; idle lanes are refilled together with one atomic
-// per warp once kRefill of them are waiting.
-constexpr int kRefill = 8;
+// the `in` queue, hit records out) or the shadow rays (ANY = true, one
+// visibility byte each).  A lane that finishes its ray takes the next one;
+// idle lanes are refilled together with one atomic per warp once kRefill of
+// them are waiting (12 of 32: 8, 10 and 16 were slower).
+constexpr int kRefill = 12;
 
 // Occupancy (measured best): 7 blocks of 128 per SM (72 registers) for
 // any-hit queries, 5 (96 registers, no spills with the row-wise box test and
