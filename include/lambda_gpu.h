@@ -461,7 +461,7 @@ int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
 
 /* lgpu_build_bvh on the context's GPU (bvh::build, cg.hpp:632-749, one
    tree level per step): the same arguments, host arrays in and out, and a
-   bit-identical result.  For hosts that load large meshes without the
+   bit-identical result.  Vertex positions must be finite.  For hosts that load large meshes without the
    reference's trimeshdata, so that building their trees does not cost a
    serial host pass per mesh. */
 int lgpu_build_bvh_device(lgpu_ctx* ctx, const float* V, uint32_t n_positions,

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 #include <string>
@@ -1054,6 +1055,11 @@ int lgpu_build_bvh_device(lgpu_ctx* ctx, const float* V, uint32_t n_positions, c
     for (int k = 0; k < 3; k++)
       if (F[size_t(f) * f_stride + k] >= n_positions)
         return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "face " + std::to_string(f) + ": vertex index out of range");
+  // the reduction that reproduces the host's nl::min / nl::max folds
+  // assumes ordered values
+  for (size_t i = 0; i < 3 * size_t(n_positions); i++)
+    if (!std::isfinite(V[i]))
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "vertex " + std::to_string(i / 3) + " is not finite");
   if (int r = bind_device(ctx)) return r;
   RefBvh B;
   cudaError_t e;

@@ -88,3 +88,7 @@ def test_device_build_rejects_bad_faces(ctx):
     F[3, 1] = V.shape[0]
     with pytest.raises(L.LgpuError):
         ctx.build_bvh(V, F, device=True)
+    V, F = _soup(10, 2)
+    V[5, 1] = np.nan
+    with pytest.raises(L.LgpuError):
+        ctx.build_bvh(V, F, device=True)
