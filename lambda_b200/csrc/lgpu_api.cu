@@ -70,6 +70,7 @@ struct lgpu_ctx {
   lgpu_stats stats{};
   // the scene table (lgpu_upload_scenes); S is a copy of slot 0's DevScene
   std::vector<SceneSlot> slots;
+  HostLayout layout;  // host side of the last upload (its arrays are reused)
   // batch tables (lgpu_render_batch)
   DevArray<DevJob> jobs;
   DevArray<uint64_t> job_items;
@@ -119,8 +120,8 @@ int cuda_fail(lgpu_ctx* ctx, cudaError_t e, const char* what) {
 }
 
 // Copies h into d, reusing d's allocation when it is large enough.
-template <class T>
-cudaError_t upload(DevArray<T>& d, const std::vector<T>& h, cudaStream_t st) {
+template <class T, class Alloc>
+cudaError_t upload(DevArray<T>& d, const std::vector<T, Alloc>& h, cudaStream_t st) {
   size_t const n = h.empty() ? 1 : h.size();
   cudaError_t e = cudaSuccess;
   if (!d.ptr || d.cap < n) {
@@ -549,7 +550,7 @@ bool timing_requested(const lgpu_render_params* p) {
 
 // Lays out one scene on the host and copies it into a scene slot.
 int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
-  HostLayout L;
+  HostLayout& L = ctx->layout;
   std::string err;
   int const rc = make_layout(scene, L, err);
   if (rc != LGPU_OK) return fail(ctx, rc, err);

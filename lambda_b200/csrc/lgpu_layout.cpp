@@ -201,80 +201,6 @@ inline bool ref_leaf(uint32_t data) { return (data & 1u) != 0; }
 inline uint32_t ref_idx(uint32_t data) { return (data & 0xFFFFFFF0u) >> 4; }
 inline uint32_t ref_count(uint32_t data) { return ((data & 0xEu) >> 1) + 1; }
 
-// Re-lays a reference-format wide BVH into WideNodes appended to `nodes`.
-// Leaf children point at slot_base + (first primitive position).  Returns
-// the root reference through root_ref and the stack bound through max_stack.
-bool relayout(const RefView& R, uint32_t slot_base, std::vector<WideNode>& nodes, uint32_t& root_ref,
-              uint32_t& max_stack, std::string& err) {
-  if (R.n_nodes == 0) {
-    err = "BVH has no nodes";
-    return false;
-  }
-  uint32_t const node_base = uint32_t(nodes.size());
-  std::vector<uint32_t> wide(R.n_nodes, 0xFFFFFFFFu);
-  uint32_t n_int = 0;
-  for (uint32_t r = 0; r < R.n_nodes; r++)
-    if (!ref_leaf(R.nodes[2 * size_t(r) + 1])) wide[r] = node_base + n_int++;
-  if (size_t(node_base) + n_int >= size_t(kLeafBit)) {
-    err = "too many BVH nodes";
-    return false;
-  }
-  auto ref_of = [&](uint32_t q, uint32_t& out) -> bool {
-    uint32_t const d = R.nodes[2 * size_t(q) + 1];
-    if (!ref_leaf(d)) {
-      out = wide[q];
-      return true;
-    }
-    uint32_t const start = ref_idx(d), cnt = ref_count(d);
-    if (size_t(start) + cnt > R.n_prims) {
-      err = "BVH leaf primitive range out of bounds";
-      return false;
-    }
-    if (size_t(slot_base) + start + cnt > size_t(kMaxSlots)) {
-      err = "too many leaf primitives for the device layout";
-      return false;
-    }
-    out = kLeafBit | ((cnt - 1) << 28) | (slot_base + start);
-    return true;
-  };
-  nodes.resize(size_t(node_base) + n_int);
-  std::vector<uint32_t> bound(R.n_nodes, 0);
-  for (uint32_t r = R.n_nodes; r-- > 0;) {
-    uint32_t const d = R.nodes[2 * size_t(r) + 1];
-    if (ref_leaf(d)) continue;
-    uint32_t const bbi = R.nodes[2 * size_t(r)];
-    uint32_t const first = ref_idx(d), cnt = ref_count(d);
-    if (bbi >= R.n_bbs || size_t(first) + cnt > R.n_nodes || first <= r) {
-      err = "malformed BVH node";
-      return false;
-    }
-    const float* bb = R.bbs + 48 * size_t(bbi);
-    WideNode& wn = nodes[wide[r]];
-    uint32_t deepest = 0;
-    for (int c = 0; c < 8; c++) {
-      if (uint32_t(c) < cnt) {
-        wn.lox[c] = bb[0 * 8 + c];
-        wn.loy[c] = bb[1 * 8 + c];
-        wn.loz[c] = bb[2 * 8 + c];
-        wn.hix[c] = bb[3 * 8 + c];
-        wn.hiy[c] = bb[4 * 8 + c];
-        wn.hiz[c] = bb[5 * 8 + c];
-        if (!ref_of(first + c, wn.child[c])) return false;
-        deepest = std::max(deepest, bound[first + c]);
-      } else {
-        wn.lox[c] = wn.loy[c] = wn.loz[c] = 1e30f;
-        wn.hix[c] = wn.hiy[c] = wn.hiz[c] = -1e30f;
-        wn.child[c] = kEmptyChild;
-      }
-    }
-    // entries the DFS stack can hold below this node: all children pushed
-    bound[r] = (cnt - 1) + deepest;
-  }
-  if (!ref_of(0, root_ref)) return false;
-  max_stack = 1 + bound[0];
-  return true;
-}
-
 // Runs fn(begin, end) over [0, n) on up to hardware_concurrency threads
 // (one for small n).
 template <class F>
@@ -292,6 +218,103 @@ void parallel_for(size_t n, F fn) {
     if (b < e) ts.emplace_back([=] { fn(b, e); });
   }
   for (auto& t : ts) t.join();
+}
+
+// Re-lays a reference-format wide BVH into WideNodes appended to `nodes`.
+// Leaf children point at slot_base + (first primitive position).  Returns
+// the root reference through root_ref and the stack bound through max_stack.
+bool relayout(const RefView& R, uint32_t slot_base, BigVector<WideNode>& nodes, uint32_t& root_ref,
+              uint32_t& max_stack, std::string& err) {
+  if (R.n_nodes == 0) {
+    err = "BVH has no nodes";
+    return false;
+  }
+  uint32_t const node_base = uint32_t(nodes.size());
+  std::vector<uint32_t> wide(R.n_nodes, 0xFFFFFFFFu);
+  uint32_t n_int = 0;
+  for (uint32_t r = 0; r < R.n_nodes; r++)
+    if (!ref_leaf(R.nodes[2 * size_t(r) + 1])) wide[r] = node_base + n_int++;
+  if (size_t(node_base) + n_int >= size_t(kLeafBit)) {
+    err = "too many BVH nodes";
+    return false;
+  }
+  enum { kOk = 0, kLeafRange = 1, kSlots = 2, kMalformed = 3 };
+  // the child reference of node q (0 or an error code)
+  auto ref_of = [&](uint32_t q, uint32_t& out) -> int {
+    uint32_t const d = R.nodes[2 * size_t(q) + 1];
+    if (!ref_leaf(d)) {
+      out = wide[q];
+      return kOk;
+    }
+    uint32_t const start = ref_idx(d), cnt = ref_count(d);
+    if (size_t(start) + cnt > R.n_prims) return kLeafRange;
+    if (size_t(slot_base) + start + cnt > size_t(kMaxSlots)) return kSlots;
+    out = kLeafBit | ((cnt - 1) << 28) | (slot_base + start);
+    return kOk;
+  };
+  nodes.resize(size_t(node_base) + n_int);
+  // every interior node's WideNode, independently of the others
+  std::atomic<int> bad{kOk};
+  parallel_for(R.n_nodes, [&](size_t r0, size_t r1) {
+    for (size_t r = r0; r < r1; r++) {
+      uint32_t const d = R.nodes[2 * r + 1];
+      if (ref_leaf(d)) continue;
+      uint32_t const bbi = R.nodes[2 * r];
+      uint32_t const first = ref_idx(d), cnt = ref_count(d);
+      if (bbi >= R.n_bbs || size_t(first) + cnt > R.n_nodes || first <= r) {
+        bad = kMalformed;
+        return;
+      }
+      const float* bb = R.bbs + 48 * size_t(bbi);
+      WideNode& wn = nodes[wide[r]];
+      for (int c = 0; c < 8; c++) {
+        if (uint32_t(c) < cnt) {
+          wn.lox[c] = bb[0 * 8 + c];
+          wn.loy[c] = bb[1 * 8 + c];
+          wn.loz[c] = bb[2 * 8 + c];
+          wn.hix[c] = bb[3 * 8 + c];
+          wn.hiy[c] = bb[4 * 8 + c];
+          wn.hiz[c] = bb[5 * 8 + c];
+          if (int const e = ref_of(first + c, wn.child[c])) {
+            bad = e;
+            return;
+          }
+        } else {
+          wn.lox[c] = wn.loy[c] = wn.loz[c] = 1e30f;
+          wn.hix[c] = wn.hiy[c] = wn.hiz[c] = -1e30f;
+          wn.child[c] = kEmptyChild;
+        }
+      }
+    }
+  });
+  switch (bad.load()) {
+    case kLeafRange:
+      err = "BVH leaf primitive range out of bounds";
+      return false;
+    case kSlots:
+      err = "too many leaf primitives for the device layout";
+      return false;
+    case kMalformed:
+      err = "malformed BVH node";
+      return false;
+  }
+  // entries the DFS stack can hold below each node (all children pushed),
+  // children first: breadth-first indices grow downwards
+  std::vector<uint32_t> bound(R.n_nodes, 0);
+  for (uint32_t r = R.n_nodes; r-- > 0;) {
+    uint32_t const d = R.nodes[2 * size_t(r) + 1];
+    if (ref_leaf(d)) continue;
+    uint32_t const first = ref_idx(d), cnt = ref_count(d);
+    uint32_t deepest = 0;
+    for (uint32_t c = 0; c < cnt; c++) deepest = std::max(deepest, bound[first + c]);
+    bound[r] = (cnt - 1) + deepest;
+  }
+  if (int const e = ref_of(0, root_ref)) {
+    err = e == kLeafRange ? "BVH leaf primitive range out of bounds" : "too many leaf primitives for the device layout";
+    return false;
+  }
+  max_stack = 1 + bound[0];
+  return true;
 }
 
 bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
@@ -337,7 +360,19 @@ int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::st
 }
 
 int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
-  L = HostLayout{};
+  // empty every array but keep its capacity
+  L.objects.clear();
+  L.meshes.clear();
+  L.nodes.clear();
+  L.tris.clear();
+  L.shade.clear();
+  L.spectra.clear();
+  L.mats.clear();
+  L.lights.clear();
+  L.tlas_objects.clear();
+  L.cmf.clear();
+  L.tlas_root = L.max_stack = L.tlas_max_stack = 0;
+  for (float& b : L.tlas_bounds) b = 0.f;
   const lgpu_spectral& sp = sc.spec;
   if (sp.n_bins < 2 || !(sp.lambda_sup > sp.lambda_inf)) {
     err = "spectral discretisation needs n_bins >= 2 and lambda_sup > lambda_inf";

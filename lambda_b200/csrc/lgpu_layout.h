@@ -1,7 +1,9 @@
 // lgpu_layout.h — host-side construction of the device scene layout.
 #pragma once
 
+#include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "lambda_gpu.h"
@@ -44,12 +46,39 @@ namespace lgpu {
 cudaError_t build_bvh_device(const float* V, uint32_t n_positions, const uint32_t* F, uint32_t f_stride,
                              uint32_t n_faces, RefBvh& out, cudaStream_t st);
 
+// An allocator whose value-initialisation leaves trivial elements
+// uninitialised: the layout writes every field of its large arrays itself,
+// so growing them need not clear tens of MB first.
+template <class T>
+struct NoInitAllocator : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAllocator<U>;
+  };
+  NoInitAllocator() = default;
+  template <class U>
+  NoInitAllocator(const NoInitAllocator<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using BigVector = std::vector<T, NoInitAllocator<T>>;
+
+// The device layout of a scene.  A context keeps one and lays every upload
+// out into it, so the arrays keep their capacity (and their pages) from one
+// upload to the next.
 struct HostLayout {
   std::vector<DevObject> objects;
   std::vector<DevMesh> meshes;
-  std::vector<WideNode> nodes;
-  std::vector<TriSlot> tris;
-  std::vector<FaceShade> shade;
+  BigVector<WideNode> nodes;
+  BigVector<TriSlot> tris;
+  BigVector<FaceShade> shade;
   std::vector<float> spectra;
   std::vector<DevMaterial> mats;
   std::vector<lgpu_light> lights;
