@@ -235,7 +235,10 @@ __global__ void __launch_bounds__(256) wf_replay_generate(OneJob jobs, WaveState
 // One vertex of the replay: the same random decisions as wf_shade, the
 // visibility recorded by the primal pass, gradients accumulated.
 template <int K>
-__global__ void __launch_bounds__(128) wf_shade_adjoint(OneJob jobs, WaveState w, AdjointArgs g) {
+// 10 blocks of 128 per SM: like the forward shading, latency-bound, so more
+// warps beat fewer spills (5 blocks at 89 registers made the adjoint 5 %
+// slower).
+__global__ void __launch_bounds__(128, 10) wf_shade_adjoint(OneJob jobs, WaveState w, AdjointArgs g) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
   const DevScene& S = jobs.S;
