@@ -1053,3 +1053,117 @@ void oracle_render_rows(const lgpu_scene* sc, uint32_t spp, uint32_t max_scatter
     }
   }
 }
+
+/* ---- single functions, for pinning ------------------------------------------------------ */
+
+static ctx_t unit_ctx(const lgpu_scene* sc) {
+  ctx_t c;
+  c.sc = sc;
+  c.K = (int)sc->spec.hero_k;
+  c.nb = sc->spec.n_bins;
+  c.inf = sc->spec.lambda_inf;
+  c.sup = sc->spec.lambda_sup;
+  c.delta = (c.sup - c.inf) / (float)(c.nb - 1);
+  if (c.K > KMAX || c.nb > NBMAX) abort();
+  return c;
+}
+static hero unit_hero(const ctx_t* c, const float* lam) {
+  hero l = hzero();
+  for (int k = 0; k < c->K; k++) l.v[k] = lam[k];
+  return l;
+}
+static hitinfo unit_hit(const oracle_hit* o) {
+  hitinfo h;
+  hinfo_init(&h);
+  h.z = o->z;
+  h.p = vload(o->p);
+  h.F.x = vload(o->Fx);
+  h.F.y = vload(o->Fy);
+  h.F.z = vload(o->Fz);
+  h.gn = vload(o->gn);
+  h.front = o->front != 0;
+  h.mat = o->mat;
+  h.obj = o->obj;
+  return h;
+}
+static void unit_put(const ctx_t* c, const hero* v, float* out) {
+  for (int k = 0; k < c->K; k++) out[k] = v->v[k];
+}
+
+void oracle_unit_spectrum(const lgpu_scene* sc, uint32_t s, const float* lam, float* out) {
+  ctx_t const c = unit_ctx(sc);
+  hero const l = unit_hero(&c, lam);
+  hero const r = spec_hero(&c, (int32_t)s, &l);
+  unit_put(&c, &r, out);
+}
+
+void oracle_unit_add_hero(const lgpu_scene* sc, const float* lam, const float* v, float* out_bins) {
+  ctx_t const c = unit_ctx(sc);
+  hero const l = unit_hero(&c, lam), s = unit_hero(&c, v);
+  memset(out_bins, 0, sizeof(float) * c.nb);
+  add_hero(&c, out_bins, &l, &s);
+}
+
+void oracle_unit_bxdf(const lgpu_scene* sc, uint32_t mat, const float* lam, const float* i,
+                      const float* o, const float* n, int front, float* out) {
+  ctx_t const c = unit_ctx(sc);
+  hero const l = unit_hero(&c, lam);
+  hero const r = bxdf(&c, &sc->materials[mat], &l, vload(i), vload(o), vload(n), front);
+  unit_put(&c, &r, out);
+}
+
+float oracle_unit_prob_for_material(const lgpu_scene* sc, float l0, const oracle_hit* h,
+                                    const float* i, const float* o, float p) {
+  ctx_t const c = unit_ctx(sc);
+  hitinfo const hh = unit_hit(h);
+  return prob_for_material(&c, &sc->materials[hh.mat], l0, &hh, vload(i), vload(o), p);
+}
+
+int oracle_unit_sample_material(const lgpu_scene* sc, const float* lam, const oracle_hit* h,
+                                const float* o, uint64_t seed, float p, float* prob, float* dir,
+                                float* mult) {
+  ctx_t const c = unit_ctx(sc);
+  hero const l = unit_hero(&c, lam);
+  hitinfo const hh = unit_hit(h);
+  rng_t rng;
+  rng.mode = ORACLE_RNG_MT19937;
+  mt_seed(&rng.mt, seed);
+  sinfo si;
+  si.prob = 0.f;
+  si.val = V3(0.f, 0.f, 0.f);
+  si.mult = hzero();
+  int const ok = sample_material(&c, &sc->materials[hh.mat], &l, &hh, vload(o), &rng, p, &si);
+  *prob = si.prob;
+  dir[0] = si.val.x;
+  dir[1] = si.val.y;
+  dir[2] = si.val.z;
+  unit_put(&c, &si.mult, mult);
+  return ok;
+}
+
+void oracle_unit_sample_light(const lgpu_scene* sc, uint32_t light, const float* lam,
+                              const oracle_hit* h, uint64_t seed, float* prob, float* dir,
+                              float* mult) {
+  ctx_t const c = unit_ctx(sc);
+  hero const l = unit_hero(&c, lam);
+  hitinfo const hh = unit_hit(h);
+  rng_t rng;
+  rng.mode = ORACLE_RNG_MT19937;
+  mt_seed(&rng.mt, seed);
+  sinfo si;
+  si.prob = 0.f;
+  si.val = V3(0.f, 0.f, 0.f);
+  si.mult = hzero();
+  sample_light(&c, &sc->lights[light], &l, &hh, &rng, &si);
+  *prob = si.prob;
+  dir[0] = si.val.x;
+  dir[1] = si.val.y;
+  dir[2] = si.val.z;
+  unit_put(&c, &si.mult, mult);
+}
+
+float oracle_unit_prob_for_light(const lgpu_scene* sc, uint32_t light, const float* ray6) {
+  ctx_t const c = unit_ctx(sc);
+  ray const r = mkray(vload(ray6), vload(ray6 + 3));
+  return prob_for_light(&c, &sc->lights[light], &r);
+}

@@ -50,6 +50,39 @@ void oracle_set_mt_arg_order(int right_to_left);
 
 int oracle_max_threads(void);
 
+/* Single functions of the restatement, for pinning them one by one against
+   the reference's own (K = the scene's hero_k wavelengths; random draws
+   from std::mt19937 seeded with `seed`, as nl::RNG(seed) draws them).  The
+   hit is hitinfo's fields (cg.hpp:1138-1149): z, p, F = (x, y, z), gn,
+   front, mat, obj. */
+typedef struct oracle_hit {
+  float z;
+  float p[3];
+  float Fx[3], Fy[3], Fz[3];
+  float gn[3];
+  uint32_t front, mat, obj;
+} oracle_hit;
+/* coefficientλ::operator()(heroλ) of spectrum s (cg.hpp:298-303) */
+void oracle_unit_spectrum(const lgpu_scene* sc, uint32_t s, const float* lam, float* out);
+/* coefficientλ::addHeroλ into a zero spectrum (cg.hpp:306-320) */
+void oracle_unit_add_hero(const lgpu_scene* sc, const float* lam, const float* v, float* out_bins);
+/* BxDFcosθ (cg.hpp:1088-1102) */
+void oracle_unit_bxdf(const lgpu_scene* sc, uint32_t mat, const float* lam, const float* i,
+                      const float* o, const float* n, int front, float* out);
+/* probForMateriali as src/renderer.cpp:136-137 calls it */
+float oracle_unit_prob_for_material(const lgpu_scene* sc, float l0, const oracle_hit* h,
+                                    const float* i, const float* o, float p);
+/* sample::materiali (cg.hpp:1953-1968); returns whether a sample was made */
+int oracle_unit_sample_material(const lgpu_scene* sc, const float* lam, const oracle_hit* h,
+                                const float* o, uint64_t seed, float p, float* prob, float* dir,
+                                float* mult);
+/* sample::light (cg.hpp:1717-1732) for light `light`, shadow ray included */
+void oracle_unit_sample_light(const lgpu_scene* sc, uint32_t light, const float* lam,
+                              const oracle_hit* h, uint64_t seed, float* prob, float* dir,
+                              float* mult);
+/* sample::probForLight (cg.hpp:1735-1747) for the ray (p, d) */
+float oracle_unit_prob_for_light(const lgpu_scene* sc, uint32_t light, const float* ray6);
+
 #ifdef __cplusplus
 }
 #endif

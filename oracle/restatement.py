@@ -29,6 +29,22 @@ def lib():
         L.oracle_mt_u64.argtypes = [ctypes.c_uint64, ctypes.c_uint64, _vp]
         L.oracle_set_mt_arg_order.argtypes = [ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
+        L.oracle_unit_spectrum.argtypes = [_vp, ctypes.c_uint32, _vp, _vp]
+        L.oracle_unit_spectrum.restype = None
+        L.oracle_unit_add_hero.argtypes = [_vp, _vp, _vp, _vp]
+        L.oracle_unit_add_hero.restype = None
+        L.oracle_unit_bxdf.argtypes = [_vp, ctypes.c_uint32, _vp, _vp, _vp, _vp, ctypes.c_int, _vp]
+        L.oracle_unit_bxdf.restype = None
+        L.oracle_unit_prob_for_material.argtypes = [_vp, ctypes.c_float, _vp, _vp, _vp, ctypes.c_float]
+        L.oracle_unit_prob_for_material.restype = ctypes.c_float
+        L.oracle_unit_sample_material.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.c_float,
+                                                  _vp, _vp, _vp]
+        L.oracle_unit_sample_material.restype = ctypes.c_int
+        L.oracle_unit_sample_light.argtypes = [_vp, ctypes.c_uint32, _vp, _vp, ctypes.c_uint64, _vp, _vp,
+                                               _vp]
+        L.oracle_unit_sample_light.restype = None
+        L.oracle_unit_prob_for_light.argtypes = [_vp, ctypes.c_uint32, _vp]
+        L.oracle_unit_prob_for_light.restype = ctypes.c_float
         _lib = L
     return _lib
 

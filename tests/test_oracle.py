@@ -64,3 +64,143 @@ def test_fp64_film_close_to_float_film(mixed_nls):
     a = ref.render_rows(8, 6, 0.8, 10, 14)
     b = ref.render_rows(8, 6, 0.8, 10, 14, fp64=True)
     assert np.allclose(a, b, rtol=1e-4, atol=1e-3)
+
+
+# ---- the restatement's single functions against the reference's ------------------
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def _unit_vectors(rng, n):
+    v = rng.normal(size=(n, 3))
+    return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+
+
+@pytest.fixture(scope="module")
+def unit_scene(scene_dir):
+    import os
+    from lambda_b200 import synth
+    nls = synth.mixed(os.path.join(str(scene_dir), "oracle_units"),
+                      lights=("sphere", "quaddir", "point", "direction", "ambient"), width=16, seed=5)
+    fs = flatten(load_nls(nls))
+    return fs, refharness.RefScene(nls)
+
+
+def _queries(ref, rng, n):
+    """Hero wavelengths, shading frames, hit points and directions, mostly
+    on the side of the surface the hit faces."""
+    lam = np.zeros((n, 16), np.float32)
+    for t in range(n):
+        ref.L.ref_hero(int(rng.integers(1, 2 ** 62)), lam[t].ctypes.data)
+    z = _unit_vectors(rng, n)
+    a = np.where(np.abs(z[:, :1]) < 0.9, [[1.0, 0.0, 0.0]], [[0.0, 1.0, 0.0]])
+    x = np.cross(z, a)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    F = np.concatenate([x, np.cross(z, x), z], axis=1).astype(np.float32)
+    front = rng.random(n) < 0.8
+    nz = z * np.where(front, 1.0, -1.0)[:, None]
+
+    def toward():
+        d = _unit_vectors(rng, n)
+        flip = (rng.random(n) < 0.75) & (np.sum(d * nz, axis=1) < 0)
+        d[flip] *= -1
+        return d.astype(np.float32)
+
+    p = rng.uniform([-2, -2, 0], [2, 2, 2], (n, 3)).astype(np.float32)
+    return lam, F, front, nz.astype(np.float32), p, toward(), toward()
+
+
+def _hits(F, front, p, mat):
+    hs = []
+    for t in range(len(F)):
+        h = refharness.RefHit()
+        h.z = 0.0
+        h.p[:] = p[t].tolist()
+        h.Fx[:], h.Fy[:], h.Fz[:] = F[t, 0:3].tolist(), F[t, 3:6].tolist(), F[t, 6:9].tolist()
+        h.gn[:] = F[t, 6:9].tolist()
+        h.front = int(front[t])
+        h.mat = mat
+        h.obj = 0xFFFFFFFF
+        hs.append(h)
+    return hs
+
+
+def test_unit_functions_bit_exact(unit_scene):
+    """BxDFcosθ, probForMateriali, sample::materiali, sample::light (with its
+    shadow ray), probForLight, the spectrum lookup and addHeroλ of the
+    restatement equal the reference's (oracle/_ref) bit for bit on random
+    inputs, for every material and light kind of the scene."""
+    import ctypes
+    fs, ref = unit_scene
+    O = R.lib()
+    sp = ctypes.addressof(fs.scene)
+    rng = np.random.default_rng(11)
+    n = 800
+    ref_h = ref.h
+    for m in range(fs.scene.n_materials):
+        if fs.materials[m].type not in (0, 1, 2):
+            continue
+        lam, F, front, nz, p, i, o = _queries(ref, rng, n)
+        hits = _hits(F, front, p, m)
+        a = np.zeros(16, np.float32)
+        b = np.zeros(16, np.float32)
+        for t in range(n):
+            ref.L.ref_bxdf(ref_h, m, lam[t].ctypes.data, i[t].ctypes.data, o[t].ctypes.data,
+                           nz[t].ctypes.data, int(front[t]), a.ctypes.data)
+            O.oracle_unit_bxdf(sp, m, lam[t].ctypes.data, i[t].ctypes.data, o[t].ctypes.data,
+                               nz[t].ctypes.data, int(front[t]), b.ctypes.data)
+            assert np.array_equal(_bits(a), _bits(b)), ("BxDFcosθ", m, t)
+            pr = ref.L.ref_prob_for_material(ref_h, float(lam[t, 0]), ctypes.byref(hits[t]),
+                                             i[t].ctypes.data, o[t].ctypes.data, 0.8)
+            po = O.oracle_unit_prob_for_material(sp, float(lam[t, 0]), ctypes.byref(hits[t]),
+                                                 i[t].ctypes.data, o[t].ctypes.data, 0.8)
+            assert _bits(pr) == _bits(po), ("probForMateriali", m, t)
+            seed = int(rng.integers(1, 2 ** 62))
+            pa, pb = ctypes.c_float(), ctypes.c_float()
+            da, db = np.zeros(3, np.float32), np.zeros(3, np.float32)
+            ka = ref.L.ref_sample_material(ref_h, lam[t].ctypes.data, ctypes.byref(hits[t]), o[t].ctypes.data,
+                                           seed, 0.8, ctypes.byref(pa), da.ctypes.data, a.ctypes.data)
+            kb = O.oracle_unit_sample_material(sp, lam[t].ctypes.data, ctypes.byref(hits[t]), o[t].ctypes.data,
+                                               seed, 0.8, ctypes.byref(pb), db.ctypes.data, b.ctypes.data)
+            assert (ka != 0) == (kb != 0), ("sample::materiali", m, t)
+            if ka:
+                assert _bits(pa.value) == _bits(pb.value) and np.array_equal(_bits(da), _bits(db)), \
+                    ("sample::materiali", m, t)
+                assert np.array_equal(_bits(a), _bits(b)), ("sample::materiali mult", m, t)
+    for li in range(fs.scene.n_lights):
+        lam, F, front, nz, p, i, o = _queries(ref, rng, n)
+        hits = _hits(F, front, p, 0)
+        a = np.zeros(16, np.float32)
+        b = np.zeros(16, np.float32)
+        for t in range(n):
+            seed = int(rng.integers(1, 2 ** 62))
+            pa, pb = ctypes.c_float(), ctypes.c_float()
+            da, db = np.zeros(3, np.float32), np.zeros(3, np.float32)
+            ref.L.ref_sample_light(ref_h, li, lam[t].ctypes.data, ctypes.byref(hits[t]), seed,
+                                   ctypes.byref(pa), da.ctypes.data, a.ctypes.data)
+            O.oracle_unit_sample_light(sp, li, lam[t].ctypes.data, ctypes.byref(hits[t]), seed,
+                                       ctypes.byref(pb), db.ctypes.data, b.ctypes.data)
+            assert _bits(pa.value) == _bits(pb.value), ("sample::light prob", li, t)
+            assert np.array_equal(_bits(da), _bits(db)) and np.array_equal(_bits(a), _bits(b)), \
+                ("sample::light", li, t)
+            ray6 = np.concatenate([p[t], i[t]]).astype(np.float32)
+            assert _bits(ref.L.ref_prob_for_light(ref_h, li, ray6.ctypes.data)) == \
+                _bits(O.oracle_unit_prob_for_light(sp, li, ray6.ctypes.data)), ("probForLight", li, t)
+    lam, *_ = _queries(ref, rng, 200)
+    for s in range(fs.scene.n_spectra):
+        v = np.ascontiguousarray(fs.spectra[s], np.float32)
+        a = np.zeros(16, np.float32)
+        b = np.zeros(16, np.float32)
+        for t in range(len(lam)):
+            ref.L.ref_eval_spectrum(v.ctypes.data, lam[t].ctypes.data, a.ctypes.data)
+            O.oracle_unit_spectrum(sp, s, lam[t].ctypes.data, b.ctypes.data)
+            assert np.array_equal(_bits(a), _bits(b)), ("spectrum", s, t)
+    nb = int(fs.scene.spec.n_bins)
+    for t in range(len(lam)):
+        val = rng.uniform(0, 3, 16).astype(np.float32)
+        a = np.zeros(nb, np.float32)
+        b = np.zeros(nb, np.float32)
+        ref.L.ref_add_hero(lam[t].ctypes.data, val.ctypes.data, a.ctypes.data)
+        O.oracle_unit_add_hero(sp, lam[t].ctypes.data, val.ctypes.data, b.ctypes.data)
+        assert np.array_equal(_bits(a), _bits(b)), ("addHeroλ", t)
