@@ -33,7 +33,9 @@
 extern "C" {
 #endif
 
-#define LGPU_ABI_VERSION 1
+/* 2: lgpu_stats gained order_rays; lgpu_probe_shading and
+   lgpu_build_bvh_device were added */
+#define LGPU_ABI_VERSION 2
 
 typedef struct lgpu_ctx lgpu_ctx;
 

@@ -194,7 +194,7 @@ def lib():
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    if L.lgpu_abi_version() != 1:
+    if L.lgpu_abi_version() != 2:
         raise RuntimeError("liblambda_gpu.so ABI version mismatch")
     _lib = L
     return L
