@@ -83,3 +83,9 @@ def test_no_device_here_is_reported():
     lib = L.lib()
     h = ctypes.c_void_p()
     assert lib.lgpu_create(0, ctypes.byref(h)) == L.ERR_NO_DEVICE
+
+
+def test_abi_version_matches_header():
+    src = open(os.path.join(REPO, "include", "lambda_gpu.h")).read()
+    v = int(re.search(r"#define LGPU_ABI_VERSION (\d+)", src).group(1))
+    assert L.lib().lgpu_abi_version() == v
