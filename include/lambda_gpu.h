@@ -34,8 +34,10 @@ extern "C" {
 #endif
 
 /* 2: lgpu_stats gained order_rays; lgpu_probe_shading and
-   lgpu_build_bvh_device were added */
-#define LGPU_ABI_VERSION 2
+   lgpu_build_bvh_device were added.
+   3: lgpu_stats gained local_stack; lgpu_trace_any was added;
+   lgpu_trace_closest runs the render's traversal kernels */
+#define LGPU_ABI_VERSION 3
 
 typedef struct lgpu_ctx lgpu_ctx;
 
@@ -246,6 +248,10 @@ typedef struct lgpu_stats {
      reference's object order (more than one mesh whose bounds contain the
      ray origin), re-traced with its linear object loop */
   uint64_t order_rays;
+  /* 1 if a traversal stack of the last render or trace grew past the 16
+     entries per ray kept in shared memory into local memory */
+  uint32_t local_stack;
+  uint32_t reserved;
 } lgpu_stats;
 
 /* Context.  `device` is a CUDA ordinal. */
@@ -355,9 +361,25 @@ int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_
                         lgpu_wave_config* out);
 
 /* intersect::scene (cg.hpp:1469-1489) on n rays given as 6 floats each
-   (origin xyz, direction xyz) in host memory; writes n lgpu_hit. */
+   (origin xyz, direction xyz) in host memory; writes n lgpu_hit.  The
+   rays run through the render's own closest-hit kernels (the persistent
+   instance-BVH traversal with its object-order fallback, or with
+   LGPU_FLAG_REFERENCE_ORDER the linear object loop), so this is the parity
+   probe of the traversal every render uses. */
 int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n,
                        uint32_t flags, lgpu_hit* out);
+
+/* Shadow-ray queries: intersect::scene(sc, ray, hinfo, skip) with hinfo.z
+   preset to tmax[i] and an object skip[i] to ignore (UINT32_MAX: none), as
+   sample::quaddirlight and sample::spherelight call it (cg.hpp:1652-1656,
+   1697-1701).  out_hit[i] = 1 if the reference's call returns true (the
+   light is occluded), else 0.  Runs the render's shadow-ray kernel (the
+   persistent any-hit traversal, or with LGPU_FLAG_REFERENCE_ORDER the
+   linear object loop).  Host buffers: rays 6*n floats, tmax n floats, skip n
+   words, out_hit n bytes. */
+int lgpu_trace_any(lgpu_ctx* ctx, const float* rays, const float* tmax,
+                   const uint32_t* skip, uint64_t n, uint32_t flags,
+                   uint8_t* out_hit);
 
 /* Unit probe of the device's shading functions (the parity probe for
    materials and lights, as lgpu_trace_closest is for hits).  Each query
@@ -420,7 +442,8 @@ int lgpu_probe_shading(lgpu_ctx* ctx, const lgpu_probe* queries, uint64_t n,
 
 /* Renderer::toneMap (src/renderer.cpp:149-176) followed by the 8-bit sRGB
    encode of rendering::rgb24 (include/renderer.hpp:20-29).  Either output
-   may be NULL.  Host buffers of w*h*3 elements. */
+   may be NULL.  Host buffers of w*h*3 elements; LGPU_ERR_TOO_LARGE if w*h
+   is beyond 2^40. */
 int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h,
                  float y_mid, float* out_tonemapped, uint8_t* out_rgb24);
 
@@ -442,7 +465,10 @@ int lgpu_get_stats(const lgpu_ctx* ctx, lgpu_stats* out);
    Every slot a call reads is written by that call first, so nothing needs
    clearing between calls.  The first call on each device looks up the
    array's device address (cudaGetSymbolAddress) with that device current;
-   make that first call before any stream capture.
+   make that first call before any stream capture.  The address is kept for
+   the life of the process: it belongs to the CUDA runtime's primary context
+   of the device, so the caller must not cudaDeviceReset that device while
+   the library is loaded.
    Limit: w*h <= LGPU_NOALLOC_MAX_PIXELS, else LGPU_ERR_TOO_LARGE. */
 #define LGPU_NOALLOC_MAX_PIXELS (1ull << 31)
 #define LGPU_NOALLOC_SCRATCH_BYTES 9728

@@ -138,7 +138,8 @@ class Stats(ctypes.Structure):
                 ("upload_bytes", ctypes.c_uint64), ("kernel_ms", ctypes.c_double * 3),
                 ("kernel_launches", ctypes.c_uint64 * 3), ("kernel_rays", ctypes.c_uint64 * 3),
                 ("kernel_node_tests", ctypes.c_uint64 * 3), ("kernel_tri_tests", ctypes.c_uint64 * 3),
-                ("kernel_inst_tests", ctypes.c_uint64 * 3), ("order_rays", ctypes.c_uint64)]
+                ("kernel_inst_tests", ctypes.c_uint64 * 3), ("order_rays", ctypes.c_uint64),
+                ("local_stack", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 FLAG_KERNEL_TIMING = 0x4
 KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2
@@ -165,6 +166,7 @@ SIGNATURES = {
     "lgpu_autotune_batch": (ctypes.c_int, [_vp, ctypes.POINTER(Job), ctypes.c_uint32, ctypes.c_uint32,
                                            ctypes.POINTER(WaveConfig)]),
     "lgpu_trace_closest": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),
+    "lgpu_trace_any": (ctypes.c_int, [_vp, _vp, _vp, _vp, ctypes.c_uint64, ctypes.c_uint32, _vp]),
     "lgpu_probe_shading": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, _vp]),
     "lgpu_tonemap": (ctypes.c_int, [_vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                     _vp, _vp]),
@@ -176,6 +178,9 @@ SIGNATURES = {
     "lgpu_build_bvh_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
                                              _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
 }
+
+# LGPU_ABI_VERSION of include/lambda_gpu.h
+ABI_VERSION = 3
 
 _lib = None
 
@@ -194,7 +199,7 @@ def lib():
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    if L.lgpu_abi_version() != 2:
+    if L.lgpu_abi_version() != ABI_VERSION:
         raise RuntimeError("liblambda_gpu.so ABI version mismatch")
     _lib = L
     return L

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "liblambda_gpu.so")
 BUILD_DIR = os.path.join(HERE, "_build")
 
-CU_SOURCES = ["lgpu_api.cu", "lgpu_kernels.cu", "lgpu_render_k4.cu", "lgpu_render_k8.cu",
+CU_SOURCES = ["lgpu_api.cu", "lgpu_kernels.cu", "lgpu_trace.cu", "lgpu_render_k4.cu", "lgpu_render_k8.cu",
               "lgpu_render_k16.cu", "lgpu_batch_k4.cu", "lgpu_batch_k8.cu", "lgpu_batch_k16.cu",
               "lgpu_adjoint_k4.cu", "lgpu_adjoint_k8.cu", "lgpu_adjoint_k16.cu",
               "lgpu_noalloc.cu", "lgpu_probe.cu", "lgpu_bvh_build.cu"]

@@ -84,6 +84,11 @@ struct lgpu_ctx {
   uint32_t* h_ctl = nullptr;  // pinned
   DevArray<float> rays;
   DevArray<lgpu_hit> hits;
+  // ray-set queries: their queue (lgpu_trace.cu) and shadow-ray inputs
+  DevArray<uint8_t> trace_arena;
+  DevArray<float> trace_tmax;
+  DevArray<uint32_t> trace_skip;
+  DevArray<uint8_t> trace_any;
   DevArray<lgpu_probe> probes;
   DevArray<lgpu_probe_result> probe_out;
   DevArray<double> partials;
@@ -188,12 +193,13 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
   }
   ctx->stats.rays = c.rays;
   ctx->stats.paths = c.paths;
-  ctx->stats.device_checks = c.flags;
+  ctx->stats.device_checks = c.flags & kTravOverflow;
   ctx->stats.node_tests = c.nodes;
   ctx->stats.tri_tests = c.tris;
   ctx->stats.inst_tests = c.insts;
   ctx->stats.nonfinite_paths = c.nonfinite;
   ctx->stats.order_rays = c.ordered;
+  ctx->stats.local_stack = (c.flags & kTravLocalStack) ? 1u : 0u;
   ctx->stats.launches = uint32_t(ctx->launch.total);
   for (int k = 0; k < 3; k++) {
     ctx->stats.kernel_ms[k] = timed ? ctx->launch.ms[k] : 0.0;
@@ -206,7 +212,7 @@ int collect(lgpu_ctx* ctx, const char* what, bool timed = false) {
     ctx->stats.kernel_tri_tests[k] = s.tris;
     ctx->stats.kernel_inst_tests[k] = s.insts;
   }
-  if (c.flags & 1u)
+  if (c.flags & kTravOverflow)
     return fail(ctx, LGPU_ERR_DEVICE_CHECK,
                 std::string(what) + ": a traversal stack bound was exceeded; results are incomplete");
   return LGPU_OK;
@@ -955,26 +961,74 @@ int lgpu_autotune_batch(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, uint32_
   return LGPU_OK;
 }
 
-int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {
-  if (!ctx || (n && (!rays || !out))) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+}  // extern "C"
+
+namespace {
+
+// lgpu_trace_closest / lgpu_trace_any: the rays in chunks of at most
+// kTraceChunk through the render's traversal kernels (lgpu_trace.cu).
+constexpr uint64_t kTraceChunk = uint64_t(1) << 22;
+
+int trace_impl(lgpu_ctx* ctx, const float* rays, const float* tmax, const uint32_t* skip, uint64_t n,
+               uint32_t flags, lgpu_hit* out, uint8_t* out_any) {
+  bool const any = out_any != nullptr;
   if (int r = bind_device(ctx)) return r;
   if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
   if (n == 0) return LGPU_OK;
-  cudaError_t e = ensure(ctx->rays, 6 * n);
-  if (e == cudaSuccess) e = ensure(ctx->hits, n);
+  uint32_t const cap = uint32_t(n < kTraceChunk ? n : kTraceChunk);
+  WaveState w{};
+  size_t const bytes = trace_wave_layout(nullptr, cap, w);
+  cudaError_t e = ensure(ctx->trace_arena, bytes);
+  if (e == cudaSuccess) e = ensure(ctx->rays, 6 * size_t(cap));
+  if (e == cudaSuccess && !any) e = ensure(ctx->hits, cap);
+  if (e == cudaSuccess && any) e = ensure(ctx->trace_tmax, cap);
+  if (e == cudaSuccess && any) e = ensure(ctx->trace_skip, cap);
+  if (e == cudaSuccess && any) e = ensure(ctx->trace_any, cap);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "ray buffers");
+  trace_wave_layout(ctx->trace_arena.ptr, cap, w);
   cudaStream_t const st = ctx->stream;
-  e = cudaMemcpyAsync(ctx->rays.ptr, rays, 6 * n * sizeof(float), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
+  e = cudaMemsetAsync(ctx->counters, 0, 3 * sizeof(DevCounters), st);
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, st);
   ctx->launch.reset(false);
-  ctx->launch.total = 1;
-  if (e == cudaSuccess) e = launch_trace(ctx->S, ctx->rays.ptr, n, flags, ctx->hits.ptr, ctx->counters, st);
+  uint64_t const chunks = (n + cap - 1) / cap;
+  // setup, load, store + the traversal (persistent + fallback, or linear)
+  ctx->launch.total = chunks * (any ? 4 : ((flags & LGPU_FLAG_REFERENCE_ORDER) || ctx->S.n_objects <= 4 ? 4 : 5));
+  for (uint64_t c0 = 0; c0 < n && e == cudaSuccess; c0 += cap) {
+    uint32_t const m = uint32_t(n - c0 < cap ? n - c0 : cap);
+    e = cudaMemcpyAsync(ctx->rays.ptr, rays + 6 * c0, 6 * size_t(m) * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && any)
+      e = cudaMemcpyAsync(ctx->trace_tmax.ptr, tmax + c0, m * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && any)
+      e = cudaMemcpyAsync(ctx->trace_skip.ptr, skip + c0, m * sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = launch_trace_chunk(ctx->S, w, ctx->rays.ptr, ctx->trace_tmax.ptr, ctx->trace_skip.ptr, m, any, flags,
+                             ctx->hits.ptr, ctx->trace_any.ptr, ctx->cfg, ctx->counters, st);
+    if (e == cudaSuccess && !any)
+      e = cudaMemcpyAsync(out + c0, ctx->hits.ptr, m * sizeof(lgpu_hit), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && any)
+      e = cudaMemcpyAsync(out_any + c0, ctx->trace_any.ptr, m, cudaMemcpyDeviceToHost, st);
+    // the staging buffers are reused by the next chunk
+    if (e == cudaSuccess && c0 + cap < n) e = cudaStreamSynchronize(st);
+  }
   if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(out, ctx->hits.ptr, n * sizeof(lgpu_hit), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "trace");
   return collect(ctx, "trace");
+}
+
+}  // namespace
+
+extern "C" {
+
+int lgpu_trace_closest(lgpu_ctx* ctx, const float* rays, uint64_t n, uint32_t flags, lgpu_hit* out) {
+  if (!ctx || (n && (!rays || !out))) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  return trace_impl(ctx, rays, nullptr, nullptr, n, flags, out, nullptr);
+}
+
+int lgpu_trace_any(lgpu_ctx* ctx, const float* rays, const float* tmax, const uint32_t* skip, uint64_t n,
+                   uint32_t flags, uint8_t* out_hit) {
+  if (!ctx || (n && (!rays || !tmax || !skip || !out_hit)))
+    return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
+  return trace_impl(ctx, rays, tmax, skip, n, flags, nullptr, out_hit);
 }
 
 int lgpu_probe_shading(lgpu_ctx* ctx, const lgpu_probe* queries, uint64_t n, lgpu_probe_result* out) {
@@ -1018,8 +1072,11 @@ int lgpu_tonemap(lgpu_ctx* ctx, const float* linrgb, uint64_t w, uint64_t h, flo
                  float* out_tonemapped, uint8_t* out_rgb24) {
   if (!ctx || !linrgb) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "null argument");
   if (int r = bind_device(ctx)) return r;
+  if (w == 0 || h == 0) return LGPU_OK;
+  // 3*w*h elements must not wrap around in the sizes below
+  if (w > (uint64_t(1) << 40) || h > (uint64_t(1) << 40) / w)
+    return fail(ctx, LGPU_ERR_TOO_LARGE, "tone map: w*h is beyond 2^40 pixels");
   uint64_t const n = w * h;
-  if (n == 0) return LGPU_OK;
   cudaStream_t const st = ctx->stream;
   uint32_t const nb = tonemap_partials_needed(n);
   cudaError_t e = ensure(ctx->partials, nb);

@@ -243,7 +243,7 @@ struct StackEntry {
   float t;
 };
 
-// Per-thread traversal counters: flags (bit 0: a stack bound was hit) and
+// Per-thread traversal counters: flags (kTravOverflow, kTravLocalStack) and
 // the work done, for the roofline's algorithmic byte count.
 struct TravStats {
   uint32_t flags;

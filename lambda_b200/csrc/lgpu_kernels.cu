@@ -9,50 +9,10 @@ namespace lgpu {
 
 namespace {
 
-// intersect::scene on a ray set (cg.hpp:1469-1489)
-__global__ void __launch_bounds__(128) trace_kernel(DevScene S, const float* __restrict__ rays, uint64_t n,
-                                                    uint32_t flags, lgpu_hit* __restrict__ out,
-                                                    DevCounters* cnt) {
-  uint64_t const i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  TravStats ts{0u, 0u, 0u, 0u};
-  if (i < n) {
-    const float* q = rays + 6 * i;
-    Ray const r = make_ray(mk(q[0], q[1], q[2]), mk(q[3], q[4], q[5]));
-    HitRec h;
-    h.z = kFltMax;
-    h.obj = UINT32_MAX;
-    h.face = UINT32_MAX;
-    StackEntry stack[kStackCap];
-    StackEntry tstack[kTlasStackCap];
-    bool const ref_order = (flags & LGPU_FLAG_REFERENCE_ORDER) != 0;
-    lgpu_hit o;
-    if (scene_hit<false>(S, r, h, UINT32_MAX, ref_order, stack, tstack, ts)) {
-      HitInfo const H = finalize_hit(S, r, h);
-      o.t = H.z;
-      o.obj = H.obj;
-      o.face = H.face;
-      o.mat = H.mat;
-      o.p[0] = H.p.x; o.p[1] = H.p.y; o.p[2] = H.p.z;
-      o.n[0] = H.F.z.x; o.n[1] = H.F.z.y; o.n[2] = H.F.z.z;
-      o.gn[0] = H.gn.x; o.gn[1] = H.gn.y; o.gn[2] = H.gn.z;
-      o.front = H.front ? 1u : 0u;
-    } else {
-      o.t = h.z;
-      o.obj = UINT32_MAX;
-      o.face = UINT32_MAX;
-      o.mat = UINT32_MAX;
-      for (int k = 0; k < 3; k++) o.p[k] = o.n[k] = o.gn[k] = 0.f;
-      o.front = 0;
-    }
-    out[i] = o;
-  }
-  flush_counters(cnt, i < n ? 1u : 0u, 0u, ts, 0u);
-}
-
 // ---- tone map (src/renderer.cpp:149-176) -------------------------------------
 
 constexpr int kTmThreads = 256;
-constexpr uint32_t kTmMaxBlocks = 148 * 8;
+constexpr uint32_t kTmMaxBlocks = kTonemapMaxPartials;
 
 // log-average luminance: per-block sums of log(max(Y, ε)) in double
 __global__ void __launch_bounds__(kTmThreads) tm_logsum_kernel(const float* __restrict__ rgb, uint64_t n,
@@ -120,14 +80,6 @@ __global__ void __launch_bounds__(kTmThreads) tm_map_kernel(const float* __restr
 }
 
 }  // namespace
-
-cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
-                         lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st) {
-  if (n == 0) return cudaSuccess;
-  uint64_t const blocks = (n + 127) / 128;
-  trace_kernel<<<dim3(uint32_t(blocks)), 128, 0, st>>>(S, d_rays, n, flags, d_hits, d_cnt);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_render(const DevScene& S, const RenderArgs& a, WaveState* wave, float* d_out,
                           DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {

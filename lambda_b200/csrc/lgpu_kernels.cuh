@@ -14,7 +14,7 @@ struct DevCounters {
   unsigned long long nodes;  // wide-node child-box tests
   unsigned long long tris;   // triangle tests
   unsigned long long insts;  // object tests
-  unsigned int flags;        // bit 0: traversal stack overflow
+  unsigned int flags;        // kTravOverflow, kTravLocalStack (lgpu_intersect.cuh)
   unsigned int nonfinite;    // paths whose radiance was NaN or infinite
   unsigned long long ordered; // rays re-traced in the reference's object order
 };
@@ -97,9 +97,6 @@ struct RenderArgs {
 // lgpu_probe_shading: one thread per query (lgpu_probe.cu)
 cudaError_t launch_probe(const DevScene& S, const lgpu_probe* d_q, uint64_t n, lgpu_probe_result* d_out,
                          cudaStream_t st);
-
-cudaError_t launch_trace(const DevScene& S, const float* d_rays, uint64_t n, uint32_t flags,
-                         lgpu_hit* d_hits, DevCounters* d_cnt, cudaStream_t st);
 
 // Launch shape of the wavefront, chosen by the autotuner
 // (lgpu_autotune_batch) or set by the caller (lgpu_set_wave_config).
@@ -248,6 +245,18 @@ struct JobTable {
 };
 #endif
 
+// Ray-set queries through the render's traversal kernels (lgpu_trace.cu).
+// trace_wave_layout lays out the queue fields they use for cap rays in one
+// allocation at base (nullptr: only counts the bytes);
+// launch_trace_chunk traces n <= cap rays: closest hits into d_hits
+// (any = false) or, for shadow rays with their distance bound and object to
+// skip, whether each is occluded into d_hit_any (any = true).
+size_t trace_wave_layout(uint8_t* base, uint32_t cap, WaveState& ws);
+cudaError_t launch_trace_chunk(const DevScene& S, WaveState& w, const float* d_rays, const float* d_tmax,
+                               const uint32_t* d_skip, uint32_t n, bool any, uint32_t flags,
+                               lgpu_hit* d_hits, uint8_t* d_hit_any, const WaveConfig& cfg, DevCounters* d_cnt,
+                               cudaStream_t st);
+
 // Batched render of the jobs of `table` (n jobs, n_items work items,
 // n_pix pixels in all) with the wavefront kernels.
 cudaError_t launch_batch(uint32_t hero_k, const DevJob* d_jobs, const uint64_t* d_item_bases,
@@ -284,7 +293,10 @@ cudaError_t launch_adjoint_k(const DevScene& S, const RenderArgs& a, WaveState* 
                              WaveLaunch* run);
 
 // Tone map: partial sums of log-luminance go to d_partials (n_partials
-// doubles, at least tonemap_partials_needed(n)).
+// doubles, at least tonemap_partials_needed(n), which never exceeds
+// kTonemapMaxPartials: the reduction is grid-strided over at most 8 blocks
+// per SM of a 148-SM B200).
+constexpr uint32_t kTonemapMaxPartials = 148 * 8;
 uint32_t tonemap_partials_needed(uint64_t n_pixels);
 cudaError_t launch_tonemap(const float* d_rgb, uint64_t n_pixels, float y_mid, double* d_partials,
                            uint32_t n_partials, float* d_exposure, float* d_out_tm,

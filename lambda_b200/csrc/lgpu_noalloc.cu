@@ -3,8 +3,8 @@
 // when they call it (see include/lambda_gpu.h).
 //
 // The tone map's scratch is the per-block partial sums of log-luminance
-// (at most tonemap_partials_needed() = 1184 doubles for any image, the
-// reduction is grid-strided) and the exposure (one float).  Both live in
+// (at most kTonemapMaxPartials doubles for any image, the reduction is
+// grid-strided) and the exposure (one float).  Both live in
 // g_tonemap_scratch; host code gets its device address once per device with
 // cudaGetSymbolAddress (the symbol itself is only a host-side stand-in) and
 // passes that address to the same kernels lgpu_tonemap launches.
@@ -17,7 +17,7 @@
 
 namespace {
 
-constexpr uint32_t kPartials = 1184;  // 148 SMs x 8: the tone map's maximum block count
+constexpr uint32_t kPartials = lgpu::kTonemapMaxPartials;
 constexpr size_t kScratchDoubles = LGPU_NOALLOC_SCRATCH_BYTES / sizeof(double);
 static_assert(kScratchDoubles >= kPartials + 1, "partials + the exposure slot");
 
@@ -28,7 +28,9 @@ std::mutex g_mu;
 double* g_scratch_ptr[kMaxDevices] = {};
 
 // Device address of g_tonemap_scratch on the current device, looked up once
-// per device with that device current.
+// per device with that device current.  The address belongs to the device's
+// primary context (the runtime's); it stays valid until that context is
+// destroyed (cudaDeviceReset), after which this cache would be stale.
 int scratch_address(double** out) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LGPU_ERR_NO_DEVICE;

@@ -40,6 +40,11 @@ constexpr uint32_t kMaxSlots = 0x10000000u;
 // traversal stack entries per ray: mesh level (cg.hpp:1407) and instance level
 constexpr int kStackCap = 64;
 constexpr int kTlasStackCap = 32;
+// traversal flags reported by the kernels: a stack bound was hit (the
+// traversal stopped; an error), and a traversal stack grew past its
+// shared-memory entries into local memory (information)
+constexpr uint32_t kTravOverflow = 1u;
+constexpr uint32_t kTravLocalStack = 2u;
 
 struct alignas(16) WideNode {
   float lox[8], loy[8], loz[8];

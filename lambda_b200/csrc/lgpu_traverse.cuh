@@ -29,8 +29,13 @@ struct SplitStack {
   uint32_t stride;
   StackEntry* lm;  // local overflow
   int sp;
+  // kTravLocalStack once an entry beyond the shared part was used (merged
+  // into the thread's TravStats::flags when its work is counted)
+  uint32_t spill;
   __device__ __forceinline__ StackEntry& at(int k) {
-    return k < kSmemStack ? sm[k * stride] : lm[k - kSmemStack];
+    if (k < kSmemStack) return sm[k * stride];
+    spill = kTravLocalStack;
+    return lm[k - kSmemStack];
   }
   __device__ __forceinline__ void push(StackEntry e) { at(sp++) = e; }
   __device__ __forceinline__ StackEntry pop() { return at(--sp); }

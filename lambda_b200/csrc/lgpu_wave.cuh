@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(128) wf_trace(J jobs, WaveState w, DevCounters
   StackEntry lm[kLocalStack];
   StackEntry lstack[kStackCap];
   StackEntry ltstack[kTlasStackCap];
-  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0, 0u};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
   uint32_t const n = *w.n_in;
@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(128) wf_trace(J jobs, WaveState w, DevCounters
     rays++;
     store_hit(w, i, h);
   }
+  ts.flags |= st.spill;
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 
@@ -314,7 +315,7 @@ template <bool ANY, int K, class J>
 __global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
-  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0, 0u};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
   uint32_t const n = ANY ? w.ctl[kCtlShadow] : *w.n_in;
@@ -410,6 +411,7 @@ __global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, 
       store_hit(w, p, t.h);
     }
   }
+  ts.flags |= st.spill;
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 
@@ -704,7 +706,7 @@ __global__ void __launch_bounds__(128) wf_shadow(J jobs, WaveState w, DevCounter
   StackEntry lm[kLocalStack];
   StackEntry lstack[kStackCap];
   StackEntry ltstack[kTlasStackCap];
-  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0};
+  SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0, 0u};
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
   uint32_t const n = w.ctl[kCtlShadow];
@@ -721,6 +723,7 @@ __global__ void __launch_bounds__(128) wf_shadow(J jobs, WaveState w, DevCounter
     rays++;
     shadow_done(w, i, !occ);
   }
+  ts.flags |= st.spill;
   flush_counters(cnt, rays, 0u, ts, 0u);
 }
 

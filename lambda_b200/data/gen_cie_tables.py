@@ -21,7 +21,9 @@ import sys
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("LAMBDA_REFERENCE", "")
+    if not ref:
+        sys.exit("usage: gen_cie_tables.py <reference source tree> (or set LAMBDA_REFERENCE)")
     d = os.path.join(ref, "lib", "numli", "data")
     out = {"source": "lib/numli/data of the reference (CIE colour-matching "
                      "functions and BT.709 spectral basis)"}

@@ -29,9 +29,12 @@ class Rendering:
     def rgb24(self, ctx=None):
         """8-bit sRGB of img (linRGB2sRGB then float2byte, cg.hpp:149-162)."""
         x = self.img.astype(np.float32)
-        s = np.where(x > np.float32(0.0031308),
-                     np.float32(1.055) * np.power(x, np.float32(1 / 2.4)) - np.float32(0.055),
+        # the power only sees values of its own branch, so negative pixels
+        # raise no warning; NaN maps to 0 as the device's encode does
+        hi = np.power(np.maximum(x, np.float32(0.0031308)), np.float32(1 / 2.4))
+        s = np.where(x > np.float32(0.0031308), np.float32(1.055) * hi - np.float32(0.055),
                      np.float32(12.92) * x)
+        s = np.nan_to_num(s, nan=0.0, posinf=1.0, neginf=0.0)
         return np.clip((np.float32(255) * s + np.float32(0.5)).astype(np.int64), 0, 255).astype(np.uint8)
 
 
@@ -201,6 +204,19 @@ class Context:
                                                      ctypes.addressof(out)), "trace")
         return hits_to_numpy(out, rays.shape[0])
 
+    def trace_any(self, rays, tmax, skip, flags=0):
+        """Shadow-ray queries (lgpu_trace_any): for each ray, whether
+        intersect::scene with the distance preset to tmax and object `skip`
+        ignored (0xFFFFFFFF: none) finds a hit, i.e. the light is occluded."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 6)
+        n = rays.shape[0]
+        tmax = np.ascontiguousarray(np.broadcast_to(np.asarray(tmax, np.float32), (n,)))
+        skip = np.ascontiguousarray(np.broadcast_to(np.asarray(skip, np.uint32), (n,)))
+        out = np.zeros(max(n, 1), np.uint8)
+        L.check(self.h, self._lib.lgpu_trace_any(self.h, rays.ctypes.data, tmax.ctypes.data, skip.ctypes.data,
+                                                 n, flags, out.ctypes.data), "trace_any")
+        return out[:n].astype(bool)
+
     def build_bvh(self, V, F, device=True):
         """bvh::build of a triangle mesh (V: positions (n, 3) with the
         loader's dummy at 0, F: (n_faces, k >= 3) vertex indices first) in
@@ -249,6 +265,7 @@ class Context:
                 "nonfinite_paths": s.nonfinite_paths, "node_tests": s.node_tests,
                 "tri_tests": s.tri_tests, "inst_tests": s.inst_tests,
                 "upload_bytes": s.upload_bytes, "launches": s.launches, "order_rays": s.order_rays,
+                "local_stack": s.local_stack,
                 "kernels": [{"ms": s.kernel_ms[k], "launches": s.kernel_launches[k],
                              "rays": s.kernel_rays[k], "node_tests": s.kernel_node_tests[k],
                              "tri_tests": s.kernel_tri_tests[k],

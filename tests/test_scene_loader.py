@@ -11,7 +11,7 @@ import pytest
 
 from lambda_b200 import _lib as L
 from lambda_b200.scene import flatten, load_nls
-from oracle import refharness
+from oracle import refharness, refpath
 
 pytestmark = pytest.mark.skipif(not refharness.available(), reason="reference harness not built")
 
@@ -100,18 +100,18 @@ def test_loader_matches_reference(which, request):
     assert compare_scenes(rs, fs.scene) == []
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/bin"), reason="reference assets absent")
+@pytest.mark.skipif(not refpath.present("bin"), reason="reference assets absent")
 def test_loader_matches_reference_on_shipped_box_scene():
     """bin/scenes/box.nls: spheres, planes, RGB spectra, a sphere light."""
-    nls = "/root/reference/bin/scenes/box.nls"
+    nls = refpath.path("bin", "scenes", "box.nls")
     cwd = os.getcwd()
-    os.chdir("/root/reference/bin")
+    os.chdir(refpath.path("bin"))
     try:
         ref = refharness.RefScene(os.path.relpath(nls))
     finally:
         os.chdir(cwd)
     rs = ctypes.cast(ref.L.ref_export(ref.h), ctypes.POINTER(L.Scene)).contents
-    fs = flatten(load_nls(nls, base_dir="/root/reference/bin"))
+    fs = flatten(load_nls(nls, base_dir=refpath.path("bin")))
     assert compare_scenes(rs, fs.scene) == []
 
 
@@ -119,14 +119,14 @@ def test_cie_tables_match_reference():
     """The 80-bin CMF and BT.709 tables built from lambda_b200/data equal
     the reference's start-up tables (read from lib/numli/data when present)."""
     from lambda_b200.scene import REFERENCE_SPECTRAL, cie_tables
-    if not os.path.isdir("/root/reference/lib/numli/data"):
+    if not refpath.present("lib/numli/data"):
         pytest.skip("reference data files absent")
     import subprocess
     import sys
     code = ("import ctypes,numpy as np;L=ctypes.CDLL(%r);o=np.zeros(480,np.float32);"
             "L.ref_get_tables(ctypes.c_void_p(o.ctypes.data));print(o.tobytes().hex())"
             % refharness.LIB_EXACT)
-    out = subprocess.run([sys.executable, "-c", code], cwd="/root/reference/bin", check=True,
+    out = subprocess.run([sys.executable, "-c", code], cwd=refpath.path("bin"), check=True,
                          capture_output=True, text=True).stdout.strip()
     ref = np.frombuffer(bytes.fromhex(out), np.float32)
     mine = np.concatenate(cie_tables(REFERENCE_SPECTRAL)).astype(np.float32)
