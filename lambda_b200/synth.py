@@ -277,12 +277,14 @@ def write_indexed_obj(path, V, N, F):
 
 
 def mixed(out_dir, width=96, ar=1.25, lights=("sphere", "quaddir", "point"), seed=7,
-          subdiv=3):
+          subdiv=3, dof=None, focal=None):
     """A small scene with every object kind (sphere, plane, instanced
     trimesh), every shaded material (Lambertian, Blinn reflective/diffuse,
     Blinn refractive with a dispersive IOR, thin film) and the requested
-    light kinds (sphere, quaddir, point, direction, ambient).  Returns the
-    .nls path."""
+    light kinds (sphere, quaddir, point, direction, ambient).  With dof, a
+    thin-lens camera of that aperture focused at distance `focal` (the
+    camera's "dof" and "f", cg.hpp:2050-2051, sampled at cg.hpp:1539).
+    Returns the .nls path."""
     os.makedirs(out_dir, exist_ok=True)
     d = os.path.abspath(out_dir)
     rng = np.random.default_rng(seed)
@@ -343,6 +345,9 @@ def mixed(out_dir, width=96, ar=1.25, lights=("sphere", "quaddir", "point"), see
     scene = {"camera": {"pos": [0.0, -6.0, 2.2], "look_at": [0.0, 0.0, 0.8], "up": [0, 0, 1],
                         "fov": 45, "ar": ar, "width": width},
              "materials": mats, "objects": objs, "lights": ls}
+    if dof is not None:
+        scene["camera"]["dof"] = float(dof)
+        scene["camera"]["f"] = float(focal if focal is not None else 6.0)
     path = os.path.join(d, "scene.nls")
     with open(path, "w") as f:
         json.dump(scene, f, indent=1)

@@ -89,6 +89,12 @@ extern "C" {
 
 int ref_n_bins() { return Nλ; }
 int ref_hero_samples() { return HERO_SAMPLES; }
+// coefficientλ's compiled-in wavelength range (cg.hpp:244-245)
+void ref_lambda_range(float* out2) {
+  coefficientλ<Nλ> const probe(0.f);
+  out2[0] = probe.inf;
+  out2[1] = probe.sup;
+}
 
 // The reference fills CMF_X/Y/Z and the BT.709 basis at static
 // initialisation from relative paths (cg.hpp:329-337).  These two calls read
@@ -209,9 +215,13 @@ void ref_render(void* h, uint64_t spp, uint64_t max_scatter, float sample_p,
 // buffer row h-1-i (src/renderer.cpp:54).  With fp64 != 0
 // the per-sample 80-bin splats are accumulated in double precision and the
 // colour conversion is done in double (out64 used instead of out32).
-void ref_render_rows(void* h, uint64_t spp, uint64_t max_scatter,
-                     float sample_p, uint64_t row0, uint64_t row1, int fp64,
-                     float* out32, double* out64) {
+// ref_render_rows_seeded seeds pixel (i, j) with seed_base + i*w + j
+// instead: seed_base = w*h gives every pixel a stream disjoint from the
+// reference's own render, for an independent oracle image.
+void ref_render_rows_seeded(void* h, uint64_t spp, uint64_t max_scatter,
+                            float sample_p, uint64_t row0, uint64_t row1,
+                            int fp64, uint64_t seed_base, float* out32,
+                            double* out64) {
   auto* r = static_cast<ref_scene*>(h);
   scene const& sc = r->sc;
   Renderer rd;
@@ -224,7 +234,7 @@ void ref_render_rows(void* h, uint64_t spp, uint64_t max_scatter,
 #pragma omp parallel for collapse(2) schedule(runtime)
   for (uint64_t i = row0; i < row1; i++)
     for (uint64_t j = 0; j < w; j++) {
-      nl::RNG rng(i * w + j);
+      nl::RNG rng(seed_base + i * w + j);
       coefficientλ<Nλ> acc(0.f);
       double acc64[Nλ] = {0.0};
       for (uint64_t k = 0; k < spp; k++) {
@@ -264,6 +274,13 @@ void ref_render_rows(void* h, uint64_t spp, uint64_t max_scatter,
         out32[3 * o + 2] = c.c[2];
       }
     }
+}
+
+void ref_render_rows(void* h, uint64_t spp, uint64_t max_scatter,
+                     float sample_p, uint64_t row0, uint64_t row1, int fp64,
+                     float* out32, double* out64) {
+  ref_render_rows_seeded(h, spp, max_scatter, sample_p, row0, row1, fp64, 0,
+                         out32, out64);
 }
 
 // Renderer::tracePath (src/renderer.cpp:64-146) for one path with an RNG

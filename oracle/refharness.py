@@ -17,6 +17,16 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_EXACT = os.path.join(HERE, "_ref", "libref.so")
 LIB_FAST = os.path.join(HERE, "_ref", "libref_fast.so")
+# the same sources built at the configurations' spectral setting (4 hero
+# wavelengths, 81 bins on 380-780 nm; oracle/Makefile)
+LIB_K4_EXACT = os.path.join(HERE, "_ref", "libref_k4.so")
+LIB_K4_FAST = os.path.join(HERE, "_ref", "libref_k4_fast.so")
+
+
+def _path(fast, k4):
+    if k4:
+        return LIB_K4_FAST if fast else LIB_K4_EXACT
+    return LIB_FAST if fast else LIB_EXACT
 
 _vp = ctypes.c_void_p
 
@@ -30,6 +40,7 @@ class RefHit(ctypes.Structure):
 
 _SIGS = {
     "ref_n_bins": (ctypes.c_int, []),
+    "ref_lambda_range": (None, [_vp]),
     "ref_hero_samples": (ctypes.c_int, []),
     "ref_get_tables": (None, [_vp]),
     "ref_set_tables": (None, [_vp]),
@@ -43,6 +54,9 @@ _SIGS = {
     "ref_render": (None, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float, _vp]),
     "ref_render_rows": (None, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                                ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _vp, _vp]),
+    "ref_render_rows_seeded": (None, [_vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
+                                      ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
+                                      _vp, _vp]),
     "ref_trace_path": (None, [_vp, _vp, _vp, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_float,
                               _vp]),
     "ref_rng_flt": (None, [ctypes.c_uint64, ctypes.c_uint64, _vp]),
@@ -68,12 +82,12 @@ _SIGS = {
 _libs = {}
 
 
-def available(fast=False):
-    return os.path.exists(LIB_FAST if fast else LIB_EXACT)
+def available(fast=False, k4=False):
+    return os.path.exists(_path(fast, k4))
 
 
-def lib(fast=False):
-    path = LIB_FAST if fast else LIB_EXACT
+def lib(fast=False, k4=False):
+    path = _path(fast, k4)
     if path in _libs:
         return _libs[path]
     L = ctypes.CDLL(path)
@@ -86,21 +100,31 @@ def lib(fast=False):
     return L
 
 
+def spectral_config(L):
+    """The library's compiled-in spectral discretisation as a
+    lambda_b200.scene.SpectralConfig."""
+    from lambda_b200.scene import SpectralConfig
+    r = np.zeros(2, np.float32)
+    L.ref_lambda_range(r.ctypes.data)
+    return SpectralConfig(n_bins=L.ref_n_bins(), lambda_inf=float(r[0]), lambda_sup=float(r[1]),
+                          hero_k=L.ref_hero_samples())
+
+
 def _install_tables(L):
     """Installs the CMF/BT.709 tables if start-up found no data files."""
-    from lambda_b200.scene import cie_tables, REFERENCE_SPECTRAL
+    from lambda_b200.scene import cie_tables
     cur = np.zeros(6 * L.ref_n_bins(), np.float32)
     L.ref_get_tables(cur.ctypes.data)
     if not np.any(cur):
-        t = np.concatenate(cie_tables(REFERENCE_SPECTRAL)).astype(np.float32)
+        t = np.concatenate(cie_tables(spectral_config(L))).astype(np.float32)
         L.ref_set_tables(t.ctypes.data)
 
 
 class RefScene:
     """A scene loaded by the reference loader."""
 
-    def __init__(self, nls_path, fast=False):
-        self.L = lib(fast)
+    def __init__(self, nls_path, fast=False, k4=False):
+        self.L = lib(fast, k4)
         self.h = self.L.ref_load(os.path.abspath(nls_path).encode())
         if not self.h:
             raise RuntimeError(f"reference loader failed on {nls_path}")
@@ -141,17 +165,19 @@ class RefScene:
         self.L.ref_render(self.h, spp, max_scatter, sample_p, out.ctypes.data)
         return out
 
-    def render_rows(self, spp, max_scatter, sample_p, row0, row1, fp64=False):
-        """Scene rows [row0, row1) in scene order (not flipped)."""
+    def render_rows(self, spp, max_scatter, sample_p, row0, row1, fp64=False, seed_base=0):
+        """Scene rows [row0, row1) in scene order (not flipped).  Pixel
+        (i, j) draws from the reference's RNG seeded seed_base + i*w + j
+        (seed_base 0: Renderer::render's own streams)."""
         n = (row1 - row0) * self.width * 3
         if fp64:
             out = np.zeros(n, np.float64)
-            self.L.ref_render_rows(self.h, spp, max_scatter, sample_p, row0, row1, 1, None,
-                                   out.ctypes.data)
+            self.L.ref_render_rows_seeded(self.h, spp, max_scatter, sample_p, row0, row1, 1, seed_base,
+                                          None, out.ctypes.data)
         else:
             out = np.zeros(n, np.float32)
-            self.L.ref_render_rows(self.h, spp, max_scatter, sample_p, row0, row1, 0,
-                                   out.ctypes.data, None)
+            self.L.ref_render_rows_seeded(self.h, spp, max_scatter, sample_p, row0, row1, 0, seed_base,
+                                          out.ctypes.data, None)
         return out.reshape(row1 - row0, self.width, 3)
 
     def render_fp64(self, spp, max_scatter, sample_p):

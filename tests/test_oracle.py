@@ -15,6 +15,18 @@ from tests import raysets
 
 pytestmark = pytest.mark.skipif(not refharness.available(), reason="reference harness not built")
 
+# the reference built at its own spectral constants (16 hero wavelengths, 80
+# bins on 400-720 nm) and at the configurations' (4, 81 on 380-780 nm)
+BUILDS = [False, pytest.param(True, marks=pytest.mark.skipif(not refharness.available(k4=True),
+                                                             reason="K=4 reference build absent"))]
+
+
+def _load(nls, k4):
+    """The scene through the loader mirror with the build's spectral
+    setting, and through the reference build's own loader."""
+    ref = refharness.RefScene(nls, k4=k4)
+    return load_nls(nls, refharness.spectral_config(ref.L)), ref
+
 
 def test_mt19937_streams_match_reference():
     L = refharness.lib()
@@ -46,11 +58,12 @@ def test_intersect_bit_exact(which, request):
     assert tri.sum() > 0
 
 
+@pytest.mark.parametrize("k4", BUILDS)
 @pytest.mark.parametrize("which", ["mixed_nls", "mixed2_nls", "box_nls"])
-def test_render_bit_exact_with_reference_stream(which, request):
+def test_render_bit_exact_with_reference_stream(which, k4, request):
     nls = request.getfixturevalue(which)
-    sc = load_nls(nls)
-    ref = refharness.RefScene(nls)
+    sc, ref = _load(nls, k4)
+    assert int(sc.cfg.hero_k) == (4 if k4 else 16)
     o = R.Oracle(flatten(sc))
     R.lib().oracle_set_mt_arg_order(1)
     rows = (sc.cam.height // 3, sc.cam.height // 3 + 12)
@@ -77,14 +90,14 @@ def _unit_vectors(rng, n):
     return (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
 
 
-@pytest.fixture(scope="module")
-def unit_scene(scene_dir):
+@pytest.fixture(scope="module", params=BUILDS, ids=["k16", "k4"])
+def unit_scene(scene_dir, request):
     import os
     from lambda_b200 import synth
     nls = synth.mixed(os.path.join(str(scene_dir), "oracle_units"),
                       lights=("sphere", "quaddir", "point", "direction", "ambient"), width=16, seed=5)
-    fs = flatten(load_nls(nls))
-    return fs, refharness.RefScene(nls)
+    sc, ref = _load(nls, request.param)
+    return flatten(sc), ref
 
 
 def _queries(ref, rng, n):
@@ -204,3 +217,39 @@ def test_unit_functions_bit_exact(unit_scene):
         ref.L.ref_add_hero(lam[t].ctypes.data, val.ctypes.data, a.ctypes.data)
         O.oracle_unit_add_hero(sp, lam[t].ctypes.data, val.ctypes.data, b.ctypes.data)
         assert np.array_equal(_bits(a), _bits(b)), ("addHeroλ", t)
+
+
+def test_instanced_scene_intersect_bit_exact(scene_dir):
+    """The benchmark scene (64 instances of a 327,680-triangle displaced
+    icosphere, ground, 2 quad lights): the restatement's intersect::scene
+    against the reference's on camera and bounce rays and rays from inside
+    overlapping object bounds."""
+    from lambda_b200 import synth
+    nls = synth.instanced(str(scene_dir / "instanced_full"), n_instances=64, subdiv=7, width=1920)
+    sc = load_nls(nls)
+    ref = refharness.RefScene(nls)
+    rays = raysets.camera_rays(sc, 256, seed=31)
+    rays = np.concatenate([rays, raysets.bounce_rays(ref.intersect(rays), 32),
+                           raysets.overlap_origin_rays(sc, 20000, seed=33)])
+    h = ref.intersect(rays)
+    g = R.Oracle(flatten(sc)).intersect(rays)
+    for f in ("t", "obj", "mat", "p", "n", "gn", "front"):
+        assert np.array_equal(np.ascontiguousarray(h[f]).view(np.uint32),
+                              np.ascontiguousarray(g[f]).view(np.uint32)), f
+
+
+def test_shipped_box_fixture_reproduces_reference_rows():
+    """The fixture of bin/scenes/box.nls (tests/golden/shipped_box.py) holds
+    the whole scene: the restatement renders its stored reference rows bit
+    for bit from the stored arrays, on the reference's own streams."""
+    import ctypes
+    from tests.golden import shipped_box
+    fx, d = shipped_box.load()
+    ref_spp, _, B = (int(x) for x in d["settings"])
+    p = float(d["sample_p"][0])
+    o = R.Oracle((ctypes.addressof(fx.scene), int(fx.scene.cam.width), int(fx.scene.cam.height)))
+    R.lib().oracle_set_mt_arg_order(1)
+    for k in (0, len(d["rows"]) // 2, len(d["rows"]) - 1):
+        r = int(d["rows"][k])
+        a = o.render_rows(ref_spp, B, p, r, r + 1)[0]
+        assert np.array_equal(a.view(np.uint32), d["ref"][k].view(np.uint32)), k

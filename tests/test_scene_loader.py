@@ -91,12 +91,18 @@ def compare_scenes(rs, ms):
     return bad
 
 
+@pytest.mark.parametrize("k4", [False, pytest.param(True, marks=pytest.mark.skipif(
+    not refharness.available(k4=True), reason="K=4 reference build absent"))])
 @pytest.mark.parametrize("which", ["mixed_nls", "mixed2_nls", "box_nls"])
-def test_loader_matches_reference(which, request):
+def test_loader_matches_reference(which, k4, request):
+    """Every flattened array of the loader mirror equals the reference
+    loader's, at the reference's spectral constants and (k4) at the
+    configurations' 4 hero wavelengths, 81 bins on 380-780 nm."""
     nls = request.getfixturevalue(which)
-    ref = refharness.RefScene(nls)
+    ref = refharness.RefScene(nls, k4=k4)
     rs = ctypes.cast(ref.L.ref_export(ref.h), ctypes.POINTER(L.Scene)).contents
-    fs = flatten(load_nls(nls))
+    fs = flatten(load_nls(nls, refharness.spectral_config(ref.L)))
+    assert int(fs.scene.spec.n_bins) == (81 if k4 else 80)
     assert compare_scenes(rs, fs.scene) == []
 
 
@@ -115,19 +121,26 @@ def test_loader_matches_reference_on_shipped_box_scene():
     assert compare_scenes(rs, fs.scene) == []
 
 
-def test_cie_tables_match_reference():
-    """The 80-bin CMF and BT.709 tables built from lambda_b200/data equal
-    the reference's start-up tables (read from lib/numli/data when present)."""
-    from lambda_b200.scene import REFERENCE_SPECTRAL, cie_tables
+@pytest.mark.parametrize("k4", [False, True])
+def test_cie_tables_match_reference(k4):
+    """The CMF and BT.709 tables built from lambda_b200/data equal the
+    reference's start-up tables (read from lib/numli/data when present): 80
+    bins on 400-720 nm, and (k4) 81 bins on 380-780 nm."""
+    from lambda_b200.scene import cie_tables
     if not refpath.present("lib/numli/data"):
         pytest.skip("reference data files absent")
+    if not refharness.available(k4=k4):
+        pytest.skip("reference build absent")
     import subprocess
     import sys
-    code = ("import ctypes,numpy as np;L=ctypes.CDLL(%r);o=np.zeros(480,np.float32);"
-            "L.ref_get_tables(ctypes.c_void_p(o.ctypes.data));print(o.tobytes().hex())"
-            % refharness.LIB_EXACT)
+    path = refharness.LIB_K4_EXACT if k4 else refharness.LIB_EXACT
+    n = 6 * (81 if k4 else 80)
+    code = ("import ctypes,numpy as np;L=ctypes.CDLL(%r);o=np.zeros(%d,np.float32);"
+            "L.ref_get_tables(ctypes.c_void_p(o.ctypes.data));print(o.tobytes().hex())" % (path, n))
     out = subprocess.run([sys.executable, "-c", code], cwd=refpath.path("bin"), check=True,
                          capture_output=True, text=True).stdout.strip()
     ref = np.frombuffer(bytes.fromhex(out), np.float32)
-    mine = np.concatenate(cie_tables(REFERENCE_SPECTRAL)).astype(np.float32)
+    assert np.any(ref != 0)
+    cfg = refharness.spectral_config(refharness.lib(k4=k4))
+    mine = np.concatenate(cie_tables(cfg)).astype(np.float32)
     assert np.array_equal(ref.view(np.uint32), mine.view(np.uint32))
