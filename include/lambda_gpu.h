@@ -35,8 +35,9 @@ extern "C" {
 
 /* 2: lgpu_stats gained order_rays; lgpu_probe_shading and
    lgpu_build_bvh_device were added.
-   3: lgpu_stats gained local_stack; lgpu_trace_any was added;
-   lgpu_trace_closest runs the render's traversal kernels */
+   3: lgpu_stats gained local_stack; lgpu_trace_any and
+   LGPU_FLAG_FP64_FILM were added; lgpu_trace_closest runs the render's
+   traversal kernels */
 #define LGPU_ABI_VERSION 3
 
 typedef struct lgpu_ctx lgpu_ctx;
@@ -199,6 +200,16 @@ typedef struct lgpu_scene {
    (CUDA events around each launch) and count their traversal work apart;
    results in lgpu_stats.kernel_*.  For profiling; it adds event records. */
 #define LGPU_FLAG_KERNEL_TIMING 0x4u
+
+/* Accumulate the film in double precision, as the reference's FP64 oracle
+   film does, and write the image as W*H*3 doubles (the output buffer holds
+   doubles, twice the bytes).  Each sample's splat is still computed in
+   float; the sums over samples and the colour conversion are double.  For
+   oracle images and finite differences, where the float film's rounding
+   would hide small differences.  lgpu_render and lgpu_render_device with
+   the wavefront kernels only (LGPU_ERR_UNSUPPORTED with the megakernel, in
+   batches and for the adjoint). */
+#define LGPU_FLAG_FP64_FILM 0x8u
 
 /* Renderer settings (include/renderer.hpp:35-37) plus the device RNG seed. */
 typedef struct lgpu_render_params {

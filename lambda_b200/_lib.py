@@ -142,6 +142,7 @@ class Stats(ctypes.Structure):
                 ("local_stack", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
 
 FLAG_KERNEL_TIMING = 0x4
+FLAG_FP64_FILM = 0x8
 KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2
 
 

@@ -234,7 +234,7 @@ struct Carver {
 // wavelengths, npix pixels and a chunk of sbuf_items work items; with
 // base == nullptr it only counts the bytes.
 size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint64_t sbuf_items, bool batch,
-                   bool adjoint, WaveState& ws) {
+                   bool adjoint, bool fp64, WaveState& ws) {
   Carver c{base};
   size_t const n = cap;
   for (PathBuf* pb : {&ws.in, &ws.out}) {
@@ -263,6 +263,7 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
   ws.fb_queue = c.take<uint32_t>(n);
   ws.ctl = c.take<uint32_t>(kCtlWords);
   ws.film = c.take<float>(3 * size_t(npix));
+  ws.film64 = fp64 ? c.take<double>(3 * size_t(npix)) : nullptr;
   ws.sbuf = c.take<float>(3 * size_t(sbuf_items));
   ws.ltot = adjoint ? c.take<float>(size_t(K) * sbuf_items) : nullptr;
   ws.vis = adjoint ? c.take<uint64_t>(sbuf_items) : nullptr;
@@ -282,14 +283,14 @@ constexpr uint64_t kSbufBytes = uint64_t(1) << 33;
 // Sizes the wavefront buffers for npix pixels, n_items work items in chunks
 // of chunk_items, and fills ws.
 int ensure_wave(lgpu_ctx* ctx, uint32_t npix, uint64_t n_items, uint64_t chunk_items, bool batch,
-                WaveState& ws, bool adjoint = false) {
+                WaveState& ws, bool adjoint = false, bool fp64 = false) {
   uint32_t const K = ctx->S.hero_k;
   uint64_t const qcap = ctx->cfg.queue_cap ? ctx->cfg.queue_cap : kQueueCap;
   uint32_t const cap = uint32_t(n_items < qcap ? n_items : qcap);
-  size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, adjoint, ws);
+  size_t const bytes = wave_layout(nullptr, cap, K, npix, chunk_items, batch, adjoint, fp64, ws);
   cudaError_t const e = ensure(ctx->w_arena, bytes);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "wavefront buffers");
-  wave_layout(ctx->w_arena.ptr, cap, K, npix, chunk_items, batch, adjoint, ws);
+  wave_layout(ctx->w_arena.ptr, cap, K, npix, chunk_items, batch, adjoint, fp64, ws);
   ws.cap = cap;
   ws.npix = npix;
   ws.n_samples = 0;
@@ -333,6 +334,9 @@ RenderArgs render_args(const lgpu_render_params* p, const DevScene& S) {
 int render_scene(lgpu_ctx* ctx, const DevScene& S, const lgpu_render_params* p, float* d_out,
                  cudaStream_t st) {
   if (!p || p->spp == 0) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "spp must be >= 1");
+  bool const fp64 = (p->flags & LGPU_FLAG_FP64_FILM) != 0;
+  if (fp64 && (p->flags & LGPU_FLAG_MEGAKERNEL))
+    return fail(ctx, LGPU_ERR_UNSUPPORTED, "the FP64 film is a wavefront option (not with the megakernel)");
   RenderArgs const a = render_args(p, S);
   WaveState ws{};
   WaveState* wave = nullptr;
@@ -340,7 +344,7 @@ int render_scene(lgpu_ctx* ctx, const DevScene& S, const lgpu_render_params* p, 
     uint64_t const npix = a.pixel_count;
     uint64_t const max_ns = kSbufBytes / (12 * npix);
     uint32_t const ns = uint32_t(a.spp < max_ns ? a.spp : (max_ns ? max_ns : 1));
-    int const r = ensure_wave(ctx, a.pixel_count, npix * a.spp, npix * ns, false, ws);
+    int const r = ensure_wave(ctx, a.pixel_count, npix * a.spp, npix * ns, false, ws, false, fp64);
     if (r != LGPU_OK) return r;
     ws.n_samples = ns;
     wave = &ws;
@@ -439,6 +443,8 @@ int batch_impl(lgpu_ctx* ctx, const lgpu_job* jobs, uint32_t n, float* const* d_
     if (jobs[k].params.spp == 0)
       return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": spp must be >= 1");
     if (!d_outs[k]) return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": null output");
+    if (jobs[k].params.flags & LGPU_FLAG_FP64_FILM)
+      return fail(ctx, LGPU_ERR_UNSUPPORTED, "job " + std::to_string(k) + ": the FP64 film is for plain renders");
     uint32_t x0, r0, tw, th;
     if (!job_rect(jobs[k], ctx->slots[jobs[k].scene].S.cam, x0, r0, tw, th))
       return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "job " + std::to_string(k) + ": rectangle outside the frame");
@@ -519,6 +525,8 @@ int adjoint_impl(lgpu_ctx* ctx, const lgpu_render_params* p, const float* d_dimg
                                                 "(max_scatterings <= 62)");
   if (p->flags & LGPU_FLAG_MEGAKERNEL)
     return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "the adjoint runs on the wavefront kernels only");
+  if (p->flags & LGPU_FLAG_FP64_FILM)
+    return fail(ctx, LGPU_ERR_UNSUPPORTED, "the adjoint's primal image is a float film");
   const DevScene& S = ctx->S;
   RenderArgs const a = render_args(p, S);
   uint64_t const npix = a.pixel_count;
@@ -758,11 +766,13 @@ int lgpu_render(lgpu_ctx* ctx, const lgpu_render_params* params, float* out_linr
   if (int r = bind_device(ctx)) return r;
   if (!ctx->has_scene) return fail(ctx, LGPU_ERR_NO_SCENE, "no scene uploaded");
   size_t const n = size_t(ctx->S.cam.width) * ctx->S.cam.height * 3;
-  cudaError_t e = ensure(ctx->out, n);
+  // an FP64 film writes doubles: twice the floats
+  size_t const nf = (params && (params->flags & LGPU_FLAG_FP64_FILM)) ? 2 * n : n;
+  cudaError_t e = ensure(ctx->out, nf);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "output buffer");
   int const rc = render_impl(ctx, params, ctx->out.ptr, ctx->stream);
   if (rc != LGPU_OK) return rc;
-  e = cudaMemcpyAsync(out_linrgb, ctx->out.ptr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+  e = cudaMemcpyAsync(out_linrgb, ctx->out.ptr, nf * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "render readback");
   return collect(ctx, "render", timing_requested(params));
 }

@@ -73,6 +73,7 @@ struct WaveState {
   uint32_t* h_ctl;     // pinned host copy of ctl
   float* sbuf;         // 3 per work item of a chunk: XYZ of every (sample, pixel)
   float* film;         // 3*npix XYZ
+  double* film64;      // 3*npix XYZ in double (LGPU_FLAG_FP64_FILM), or nullptr
   // path replay (lgpu_adjoint): the primal pass records every path's
   // radiance and which of its shadow rays were unoccluded; the replay
   // pass reads them back

@@ -316,6 +316,7 @@ template <int K, class J>
 cudaError_t run_wave(const J& jobs, WaveState w, uint64_t n_items, uint64_t chunk_items, bool linear,
                      DevCounters* d_cnt, cudaStream_t st, WaveLaunch* run) {
   cudaError_t e = cudaMemsetAsync(w.film, 0, sizeof(float) * 3 * size_t(w.npix), st);
+  if (e == cudaSuccess && w.film64) e = cudaMemsetAsync(w.film64, 0, sizeof(double) * 3 * size_t(w.npix), st);
   for (uint64_t c0 = 0; c0 < n_items && e == cudaSuccess; c0 += chunk_items) {
     uint32_t const total = uint32_t(n_items - c0 < chunk_items ? n_items - c0 : chunk_items);
     e = wave_chunk<K>(jobs, w, c0, total, linear, d_cnt, st, run);

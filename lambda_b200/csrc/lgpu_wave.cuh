@@ -230,6 +230,21 @@ __global__ void __launch_bounds__(256) wf_reduce(J jobs, WaveState w, uint64_t c
     uint64_t hi = c1 > base ? (c1 - base + npix - 1) / npix : 0;
     if (hi > spp) hi = spp;
     if (lo >= hi) continue;
+    if (w.film64) {
+      // the FP64 film: the same samples in the same order, summed in double
+      double* const f = w.film64 + 3 * size_t(gp);
+      double X = f[0], Y = f[1], Z = f[2];
+      for (uint64_t s = lo; s < hi; s++) {
+        size_t const o = 3 * size_t(base + s * npix - w.c0);
+        X += double(w.sbuf[o]);
+        Y += double(w.sbuf[o + 1]);
+        Z += double(w.sbuf[o + 2]);
+      }
+      f[0] = X;
+      f[1] = Y;
+      f[2] = Z;
+      continue;
+    }
     float X = w.film[3 * size_t(gp)], Y = w.film[3 * size_t(gp) + 1], Z = w.film[3 * size_t(gp) + 2];
     for (uint64_t s = lo; s < hi; s++) {
       size_t const o = 3 * size_t(base + s * npix - w.c0);
@@ -253,6 +268,18 @@ __global__ void __launch_bounds__(256) wf_finalize(J jobs, WaveState w) {
     uint32_t const pix = jobs.frame_pixel(jb, gp - jobs.pix_base(jb));
     uint32_t const W = uint32_t(S.cam.width), H = uint32_t(S.cam.height);
     uint32_t const i = pix / W, j = pix - i * W;
+    if (w.film64) {
+      // double throughout, into an output of doubles
+      double const nd = double(jobs.args(jb).spp) * double(K);
+      double const X = w.film64[3 * size_t(gp)] / nd * double(S.lambda_delta);
+      double const Y = w.film64[3 * size_t(gp) + 1] / nd * double(S.lambda_delta);
+      double const Z = w.film64[3 * size_t(gp) + 2] / nd * double(S.lambda_delta);
+      double* o = reinterpret_cast<double*>(jobs.out_of(jb)) + (size_t(H - i - 1) * W + j) * 3;
+      o[0] = 3.2404542 * X - 1.5371385 * Y - 0.4985314 * Z;
+      o[1] = -0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z;
+      o[2] = 0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z;
+      continue;
+    }
     float const norm = float(jobs.args(jb).spp) * float(K);
     float const X = (w.film[3 * size_t(gp)] / norm) * S.lambda_delta;
     float const Y = (w.film[3 * size_t(gp) + 1] / norm) * S.lambda_delta;

@@ -152,9 +152,13 @@ class Context:
         return int(c.width), int(c.height)
 
     def render(self, spp, max_scatterings, sample_p, seed=0, flags=0, spp_offset=0, out=None):
+        """The image (height, width, 3), row 0 at the top: float32, or
+        float64 with flags containing FLAG_FP64_FILM."""
         w, h = self.size
+        dt = np.float64 if flags & L.FLAG_FP64_FILM else np.float32
         if out is None:
-            out = np.empty((h, w, 3), np.float32)
+            out = np.empty((h, w, 3), dt)
+        assert out.dtype == dt and out.flags.c_contiguous and out.size == h * w * 3
         p = L.RenderParams(spp=spp, max_scatterings=max_scatterings, sample_p=sample_p, flags=flags,
                            seed=seed, spp_offset=spp_offset)
         L.check(self.h, self._lib.lgpu_render(self.h, ctypes.byref(p), out.ctypes.data), "render")
