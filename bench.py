@@ -20,6 +20,14 @@ over ranks).  e2e: the same metric through the C ABI with host buffers —
 lgpu_upload_scene (host layout + host-to-device copies) plus lgpu_render
 (kernel + device-to-host image) per step.  Multi-GPU: every rank renders
 its own frame (weak scaling, no collective on the data path).
+
+Beside the headline (N=1, rank 0): roofline (HBM, FP32 and issue bounds of
+the dominant kernel), cpu_baseline (the reference's own pixel loop on the
+host's cores), rmse (fixed-RMSE check against the reference's FP64 film),
+batched (config 3: 64 jobs in one launch vs back to back), adjoint (config
+4: cost and finite-difference check), box_room (config 1, against the
+reference built at 4 hero wavelengths, 81 bins on 380-780 nm) and large
+(config 5: a 4K frame as 16 tile jobs, one adjoint pass).
 """
 import argparse
 import json
@@ -47,6 +55,19 @@ BYTES_PER_NODE = 200
 BYTES_PER_TRI = 36
 BYTES_PER_INST = 128
 BYTES_PER_RAY = 64
+# per-unit FP32 operations of the traversal, counted from the kernel source
+# (lgpu_intersect.cuh; every operation is one instruction, the library is
+# built without multiply-add contraction): an 8-wide node test is 8 children
+# x (6 subtractions + 6 multiplications + 3 max + 3 min + 1 compare) plus 28
+# compares ranking the hit children; a full triangle test (tri_test) 108; an
+# instance entry (two 3x4 transforms, the inverse direction, the mesh-bounds
+# slab test, the ray's moment) 80
+FLOPS_PER_NODE = 8 * 19 + 28
+FLOPS_PER_TRI = 108
+FLOPS_PER_INST = 80
+# B200: 148 SMs, 128 FP32 lanes and 4 warp schedulers (one instruction per
+# cycle each) per SM
+N_SM, FP32_LANES, SCHEDULERS = 148, 128, 4
 
 
 def workload_desc(w):
@@ -129,15 +150,15 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profile_traffic_per_ray(kind):
-    """DRAM bytes (read + write) per ray of kernel kind (0 closest-hit,
-    1 shadow) from the committed ncu summary
-    profiles/traffic_instanced.json, or None."""
+def profile_per_ray(kind, key="dram_bytes_per_ray"):
+    """A per-ray figure of kernel kind (0 closest-hit, 1 shadow) from the
+    committed ncu summary profiles/traffic_instanced.json: DRAM bytes (read
+    + write) or warp instructions issued, per traced ray; None if absent."""
     p = os.path.join(REPO, "profiles", "traffic_instanced.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return float(d["dram_bytes_per_ray"][str(kind)])
+        return float(d[key][str(kind)])
     except (OSError, KeyError, ValueError, TypeError):
         return None
 
@@ -146,13 +167,21 @@ KERNEL_NAMES = ("closest-hit traversal (wf_trace_persistent<false> + wf_trace_fa
                 "shadow traversal (wf_trace_persistent<true>)", "shading (wf_shade)")
 
 
-def kernel_roofline(ctx, spp, B, p, stream):
+def kernel_roofline(ctx, spp, B, p, stream, sm_mhz=None):
     """Roofline of the dominant kernel from one untimed render with
     per-kernel timing (CUDA events around every traversal and shading
-    launch on the render stream, separate work counters per kind).
-    achieved = algorithmic bytes of its launches / their summed device
-    time; the algorithmic bytes are its node, triangle, instance and ray
-    counts times BYTES_PER_*."""
+    launch on the render stream, separate work counters per kind), against
+    three bounds:
+      hbm    algorithmic bytes (node, triangle, instance and ray counts x
+             BYTES_PER_*) / its summed device time, against the measured
+             copy bandwidth (MEASURED_PEAKS.json);
+      fp32   algorithmic FP32 operations (FLOPS_PER_*) / time, against 148
+             SMs x 128 lanes x the SM clock sampled during the run;
+      issue  warp instructions issued (per ray, from the committed ncu
+             summary, x the rays) / time, against 148 SMs x 4 schedulers x
+             the SM clock.
+    `bound` names the largest fraction; achieved/peak/unit/frac are that
+    bound's, and every bound's figures are listed under `bounds`."""
     import torch
 
     from lambda_b200 import _lib as L
@@ -174,12 +203,36 @@ def kernel_roofline(ctx, spp, B, p, stream):
                 k["inst_tests"] * BYTES_PER_INST + k["rays"] * BYTES_PER_RAY)
         achieved = algo / (k["ms"] / 1e3) / 1e9
     launches = max(int(k["launches"]), 1)
-    tpr = profile_traffic_per_ray(top)
+    tpr = profile_per_ray(top)
     tpl = tpr * k["rays"] / launches if tpr is not None else None
-    return {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak,
-            "unit": "GB/s", "frac": (achieved / peak) if achieved is not None else None,
-            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-            else peak_kind,
+    mhz = float(sm_mhz or 1965.0)
+    secs = k["ms"] / 1e3
+    bounds = {"hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s",
+                      "frac": (achieved / peak) if achieved is not None else None,
+                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                      else peak_kind + " (6650 GB/s)"}}
+    if top != 2 and secs > 0:
+        ops = (k["node_tests"] * FLOPS_PER_NODE + k["tri_tests"] * FLOPS_PER_TRI +
+               k["inst_tests"] * FLOPS_PER_INST)
+        pk = N_SM * FP32_LANES * mhz * 1e6 / 1e12
+        bounds["fp32"] = {"achieved": ops / secs / 1e12, "peak": pk, "unit": "TFLOP/s",
+                          "frac": ops / secs / 1e12 / pk,
+                          "peak_source": "148 SMs x 128 FP32 lanes x %.0f MHz (SM clock sampled during the run); "
+                                         "no multiply-add contraction, one operation per instruction" % mhz}
+        ipr = profile_per_ray(top, "warp_inst_per_ray")
+        if ipr is not None:
+            inst = ipr * k["rays"]
+            pk = N_SM * SCHEDULERS * mhz * 1e6 / 1e12
+            bounds["issue"] = {"achieved": inst / secs / 1e12, "peak": pk, "unit": "Twarp-inst/s",
+                               "frac": inst / secs / 1e12 / pk, "warp_inst_per_ray": ipr,
+                               "peak_source": "148 SMs x 4 schedulers x %.0f MHz; instructions per ray from "
+                                              "profiles/traffic_instanced.json (ncu smsp__inst_executed.sum)"
+                                              % mhz}
+    binding = max((b for b in bounds if bounds[b]["frac"] is not None), key=lambda b: bounds[b]["frac"],
+                  default="hbm")
+    bb = bounds[binding]
+    return {"bound": binding, "kernel": KERNEL_NAMES[top], "achieved": bb["achieved"], "peak": bb["peak"],
+            "unit": bb["unit"], "frac": bb["frac"], "peak_source": bb["peak_source"], "bounds": bounds,
             "traffic": tpl,
             "algorithmic_bytes_per_launch": (algo / launches) if algo is not None else None,
             "avg_launch_ms": k["ms"] / launches, "launches": int(k["launches"]),
@@ -267,28 +320,49 @@ def run_batched(ctx_cls, device, n_jobs=64):
 
 ADJ_DESC = ("inverse-rendering scene: 64x64 thin-film tiles (one object and material each) under 64 "
             "Lambertian UV spheres (48K tris), 2 quad lights; 512x512, 32 spp, 4 bounces, p=0.8, "
-            "16 hero wavelengths 400-720 nm (80 bins); parameters 64x32 albedo samples + 64x64 thickness")
+            "16 hero wavelengths 400-720 nm (80 bins); parameters 64x32 albedo samples + 64x64 thickness; "
+            "L2 loss against a 1024-spp target rendered with hidden parameters")
+FD_H = 1e-3          # albedo samples: absolute; thickness: relative
+FD_FLOOR = 0.01      # relative errors are taken against max(|fd|, FD_FLOOR x RMS of the checked fds)
 
 
 def run_adjoint(device, n_fd=100, reps=3):
-    """Config 4: forward render vs path-replay adjoint (device time, CUDA
-    events), and the adjoint against central finite differences of the
-    device renderer with common random numbers on n_fd random parameters
-    (loss <w, image> with a fixed seeded weight image w)."""
+    """Config 4: the forward render vs the path-replay adjoint (device time,
+    CUDA events), and the adjoint against central finite differences of
+    the device renderer with common random numbers on n_fd random
+    parameters.  Loss = sum((I - T)^2) against a target T rendered at 1024
+    spp with hidden parameters (thickness U[200, 800] nm, albedo random);
+    the parameters sit at the initial guess (thickness 400 nm, albedo 0.5).
+    Finite differences render with the FP64 film (LGPU_FLAG_FP64_FILM) at
+    h = FD_H, so the float film's rounding does not swamp them."""
     import numpy as np
     import torch
 
+    from lambda_b200 import _lib as L
     from lambda_b200 import synth
     from lambda_b200.inverse import DiffScene
     rng = np.random.default_rng(4)
-    alb = rng.uniform(0.1, 0.9, (64, synth.ALBEDO_BINS))
-    th = rng.uniform(200.0, 800.0, (64, 64))
+    alb_true = np.clip(rng.uniform(0.1, 0.9, (64, 1)) + 0.1 * rng.standard_normal((64, synth.ALBEDO_BINS)),
+                       0.05, 0.95)
+    th_true = rng.uniform(200.0, 800.0, (64, 64))
+    alb = np.full((64, synth.ALBEDO_BINS), 0.5)
+    th = np.full((64, 64), 400.0)
     sc = DiffScene(alb, th, width=512, spp=32, bounces=4, device=device)
+    sc.set_params(alb_true, th_true)
+    target = sc.ctx.render(1024, sc.bounces, sc.p, seed=99, flags=L.FLAG_FP64_FILM)
     sc.set_params(alb, th)
     ctx = sc.ctx
     H, W, _ = sc.shape
-    wimg = np.random.default_rng(5).standard_normal((H, W, 3)).astype(np.float32)
-    d_w = torch.from_numpy(wimg).cuda()
+    seed = 7
+
+    def img_fp64():
+        return ctx.render(sc.spp, sc.bounces, sc.p, seed=seed, flags=L.FLAG_FP64_FILM)
+
+    def loss():
+        return float(np.sum((img_fp64() - target) ** 2))
+
+    dimg = (2.0 * (img_fp64() - target)).astype(np.float32)
+    d_w = torch.from_numpy(dimg).cuda()
     d_img = torch.empty(H * W * 3, dtype=torch.float32, device="cuda")
     n_spec = int(sc.flat.scene.n_spectra) * int(sc.flat.scene.spec.n_bins)
     d_gs = torch.empty(n_spec, dtype=torch.float32, device="cuda")
@@ -305,69 +379,64 @@ def run_adjoint(device, n_fd=100, reps=3):
         return e0.elapsed_time(e1) / 1e3
 
     def fwd():
-        ctx.render_device(sc.spp, sc.bounces, sc.p, d_img.data_ptr(), seed=7, stream=stream.cuda_stream)
+        ctx.render_device(sc.spp, sc.bounces, sc.p, d_img.data_ptr(), seed=seed, stream=stream.cuda_stream)
 
     def adj():
-        ctx.adjoint_device(sc.spp, sc.bounces, sc.p, d_w.data_ptr(), d_gs.data_ptr(), d_gm.data_ptr(), seed=7,
+        ctx.adjoint_device(sc.spp, sc.bounces, sc.p, d_w.data_ptr(), d_gs.data_ptr(), d_gm.data_ptr(), seed=seed,
                            stream=stream.cuda_stream)
 
     fwd()
     adj()
     t_f = min(timed(fwd) for _ in range(reps))
     t_a = min(timed(adj) for _ in range(reps))
-    g_alb, g_th = sc.gradients(wimg, seed=7)
+    g_alb, g_th = sc.gradients(dimg, seed=seed)
     paths = H * W * sc.spp
 
-    def loss():
-        return float(np.sum(sc.render(seed=7).astype(np.float64) * wimg))
-
-    def fd_check(h_alb, h_th_rel):
-        """central differences with the given steps on n_fd random parameters"""
-        frng = np.random.default_rng(11)
-        live_a = np.argwhere(g_alb != 0)
-        live_t = np.argwhere(g_th != 0)
-        out = []
-        for k in range(n_fd):
-            if frng.uniform() < 0.5 or len(live_t) == 0:
-                i, j = (int(x) for x in live_a[frng.integers(len(live_a))])
-                h, g = h_alb, g_alb[i, j]
-                a = alb.copy()
-                a[i, j] += h
-                sc.set_params(a, th)
-                lp = loss()
-                a[i, j] -= 2 * h
-                sc.set_params(a, th)
-                lm = loss()
-                name = "albedo"
-            else:
-                i, j = (int(x) for x in live_t[frng.integers(len(live_t))])
-                h, g = h_th_rel * th[i, j], g_th[i, j]
-                t = th.copy()
-                t[i, j] += h
-                sc.set_params(alb, t)
-                lp = loss()
-                t[i, j] -= 2 * h
-                sc.set_params(alb, t)
-                lm = loss()
-                name = "thickness"
-            out.append((name, i, j, float(g), (lp - lm) / (2 * h)))
-        sc.set_params(alb, th)
-        g = np.array([[o[3], o[4]] for o in out])
-        rel = np.abs(g[:, 0] - g[:, 1]) / np.maximum(np.abs(g[:, 1]), 1e-30)
-        worst = np.argsort(-rel)[:3]
-        return {"h": "%g (albedo) / %g x thickness" % (h_alb, h_th_rel),
-                "rel_err_median": float(np.median(rel)), "rel_err_max": float(rel.max()),
-                "within_2pct": int(np.sum(rel <= 0.02)), "worst": [list(out[w]) for w in worst],
-                "drawn_from": "%d albedo samples, %d tiles with a non-zero adjoint gradient" %
-                              (len(live_a), len(live_t))}
-
-    fd3 = fd_check(1e-3, 1e-3)
-    fd2 = fd_check(1e-2, 1e-2)
+    frng = np.random.default_rng(11)
+    live_a = np.argwhere(g_alb != 0)
+    live_t = np.argwhere(g_th != 0)
+    out = []
+    for k in range(n_fd):
+        if frng.uniform() < 0.5 or len(live_t) == 0:
+            i, j = (int(x) for x in live_a[frng.integers(len(live_a))])
+            h, g = FD_H, g_alb[i, j]
+            a = alb.copy()
+            a[i, j] += h
+            sc.set_params(a, th)
+            lp = loss()
+            a[i, j] -= 2 * h
+            sc.set_params(a, th)
+            lm = loss()
+            name = "albedo"
+        else:
+            i, j = (int(x) for x in live_t[frng.integers(len(live_t))])
+            h, g = FD_H * th[i, j], g_th[i, j]
+            t = th.copy()
+            t[i, j] += h
+            sc.set_params(alb, t)
+            lp = loss()
+            t[i, j] -= 2 * h
+            sc.set_params(alb, t)
+            lm = loss()
+            name = "thickness"
+        out.append((name, i, j, float(g), (lp - lm) / (2 * h)))
+    sc.set_params(alb, th)
+    gg = np.array([[o[3], o[4]] for o in out])
+    floor = FD_FLOOR * float(np.sqrt(np.mean(gg[:, 1] ** 2)))
+    rel = np.abs(gg[:, 0] - gg[:, 1]) / np.maximum(np.abs(gg[:, 1]), floor)
+    rel_strict = np.abs(gg[:, 0] - gg[:, 1]) / np.maximum(np.abs(gg[:, 1]), 1e-300)
+    worst = np.argsort(-rel)[:3]
     return {"forward_s": t_f, "adjoint_s": t_a, "cost_ratio": t_a / t_f,
             "forward_mpaths_s": paths / t_f / 1e6, "fd_params": n_fd,
-            "fd": "central differences of the device renderer, same seed (common random numbers), loss "
-                  "<w, image> with a seeded normal weight image; relative error |adjoint - fd| / |fd|",
-            "fd_h1e-3": fd3, "fd_h1e-2": fd2, "workload": ADJ_DESC}
+            "fd": "central differences of the device renderer with the FP64 film, same seed (common random "
+                  "numbers), h = %g (albedo samples) / %g x thickness; loss sum((I - T)^2) against a 1024-spp "
+                  "target with hidden parameters" % (FD_H, FD_H),
+            "rel_err": "|adjoint - fd| / max(|fd|, %g x RMS of the %d fds = %.3g)" % (FD_FLOOR, n_fd, floor),
+            "within_2pct": int(np.sum(rel <= 0.02)), "within_2pct_without_floor": int(np.sum(rel_strict <= 0.02)),
+            "rel_err_median": float(np.median(rel)), "rel_err_max": float(rel.max()),
+            "worst": [list(out[w]) for w in worst],
+            "drawn_from": "%d albedo samples, %d tiles with a non-zero adjoint gradient" % (len(live_a), len(live_t)),
+            "workload": ADJ_DESC}
 
 
 LARGE = dict(n_instances=256, width=3840, spp=256, bounces=32, p=0.8)
@@ -377,9 +446,13 @@ LARGE_DESC = ("large: 256 instances of a 65,536-triangle displaced UV sphere (16
               "albedo and thin-film IOR spectra, thicknesses, exponents)")
 
 
-def run_large(args):
+def run_large(spp=None, oracle_rows=2, oracle_spp=1024):
     """Config 5: the 4K frame as 16 tile jobs in one batched launch, the
-    same frame as one plain render, and one adjoint pass of it."""
+    same frame as one plain render, one adjoint pass of it, and the RMSE of
+    oracle_rows rows of the tiled frame against the reference's FP64 film
+    at oracle_spp (the reference's own rows at the frame's spp beside it).
+    Each is timed once, after a warm-up at 96 spp (tiles) and 32 spp
+    (adjoint) that sizes the same buffers."""
     import numpy as np
     import torch
 
@@ -387,8 +460,8 @@ def run_large(args):
     from lambda_b200.renderer import Context
     from lambda_b200.scene import flatten, load_nls
     w = dict(LARGE)
-    if args.spp:
-        w["spp"] = args.spp
+    if spp:
+        w["spp"] = spp
     root = os.path.join(tempfile.gettempdir(), "lgpu_bench", "large")
     nls = synth.instanced(root, n_instances=w["n_instances"], width=w["width"], mesh="uv64k")
     fs = flatten(load_nls(nls))
@@ -406,73 +479,182 @@ def run_large(args):
              for a in range(4)]
 
     def timed(fn):
-        # the second of two runs: the first also sizes the context's buffers
-        # for the call (tens of GB at this size)
-        for _ in range(2):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
         return e0.elapsed_time(e1) / 1e3
 
+    ctx.render_batch_device([dict(t, spp=min(96, w["spp"])) for t in tiles], [d_tiles.data_ptr()] * 16,
+                            stream=stream.cuda_stream)
+    t_tiles = timed(lambda: ctx.render_batch_device(tiles, [d_tiles.data_ptr()] * 16, stream=stream.cuda_stream))
     t_plain = timed(lambda: ctx.render_device(w["spp"], w["bounces"], w["p"], d_out.data_ptr(), seed=3,
                                               stream=stream.cuda_stream))
-    t_tiles = timed(lambda: ctx.render_batch_device(tiles, [d_tiles.data_ptr()] * 16, stream=stream.cuda_stream))
     same = bool(torch.equal(d_out, d_tiles))
     wimg = torch.from_numpy(np.random.default_rng(5).standard_normal(H * W * 3).astype(np.float32)).cuda()
     n_spec = int(fs.scene.n_spectra) * int(fs.scene.spec.n_bins)
     d_gs = torch.zeros(n_spec, dtype=torch.float32, device="cuda")
     d_gm = torch.zeros(4 * int(fs.scene.n_materials), dtype=torch.float32, device="cuda")
-    t_adj = timed(lambda: ctx.adjoint_device(w["spp"], w["bounces"], w["p"], wimg.data_ptr(), d_gs.data_ptr(),
-                                             d_gm.data_ptr(), seed=3, stream=stream.cuda_stream))
-    line = {"metric": METRIC, "value": paths / t_tiles / 1e6, "unit": UNIT, "n_gpus": 1, "steps": 1,
-            "warmup": 1, "ms_per_step": t_tiles * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
-            "config": {"workload": LARGE_DESC, "paths": paths},
-            "plain_value": paths / t_plain / 1e6, "tiles_identical_to_plain": same,
-            "adjoint_s": t_adj, "adjoint_cost_ratio": t_adj / t_plain,
-            "gradient_nonzero": int((d_gs != 0).sum().item() + (d_gm != 0).sum().item())}
-    print(json.dumps(line))
-    return 0
+
+    def adj(n_spp):
+        ctx.adjoint_device(n_spp, w["bounces"], w["p"], wimg.data_ptr(), d_gs.data_ptr(), d_gm.data_ptr(), seed=3,
+                           stream=stream.cuda_stream)
+    adj(min(32, w["spp"]))
+    t_adj = timed(lambda: adj(w["spp"]))
+    out = {"value": paths / t_tiles / 1e6, "unit": UNIT, "seconds": t_tiles, "paths": paths,
+           "plain_value": paths / t_plain / 1e6, "tiles_identical_to_plain": same,
+           "adjoint_s": t_adj, "adjoint_cost_ratio": t_adj / t_plain,
+           "gradient_nonzero": int((d_gs != 0).sum().item() + (d_gm != 0).sum().item()),
+           "workload": LARGE_DESC}
+    from oracle import refharness
+    if oracle_rows and refharness.available(fast=True):
+        img = d_tiles.cpu().numpy().reshape(H, W, 3).astype(np.float64)
+        ref = refharness.RefScene(nls, fast=True)
+        rows = [int(round(x)) for x in np.linspace(H * 0.3, H * 0.7, oracle_rows)]
+        t0 = time.perf_counter()
+        orc = np.stack([ref.render_rows(oracle_spp, w["bounces"], w["p"], r, r + 1, fp64=True,
+                                        seed_base=W * H)[0] for r in rows])
+        cref = np.stack([ref.render_rows(w["spp"], w["bounces"], w["p"], r, r + 1)[0] for r in rows])
+        dev = image_stats(np.stack([img[H - 1 - r] for r in rows]), orc)
+        cpu = image_stats(cref, orc)
+        out["rmse"] = {"device": dev, "reference": cpu,
+                       "ratio": [a / b for a, b in zip(dev["rel_rmse"], cpu["rel_rmse"])],
+                       "rows": rows, "oracle_seconds": time.perf_counter() - t0,
+                       "oracle": "reference FP64 film (oracle/_ref fast build), %d spp, seed base w*h, %d rows "
+                                 "of the tiled 4K frame" % (oracle_spp, len(rows))}
+    ctx.close()
+    return out
 
 
-def rmse_check(ctx, w, ref_rows, d_out, stream, oracle_renders=16):
-    """Relative RMSE per channel, over the reference's sampled rows, of the
-    device image and of the reference's own image at the workload's spp,
-    both against an FP64 mean of oracle_renders device renders of that spp
-    with other random streams (the high-spp oracle image)."""
+BOX_DESC = ("box room: unit cube of 5 walls (10 tris; white 0.75, left 0.6 above 600 nm, right 0.6 on 500-560 nm), "
+            "2 blocks (12 tris each), 0.25x0.25 ceiling quad light (blackbody 6500 K); 256x256, 16 spp, "
+            "8 bounces, p=0.8, 4 hero wavelengths on 380-780 nm (81 bins)")
+BOX = dict(width=256, spp=16, bounces=8, p=0.8)
+
+
+def run_box_room(device, steps=20, warmup=3):
+    """Config 1: the box room on the device (scene resident, CUDA events,
+    L2 flushed between renders; and end to end through the C ABI), the
+    reference built at the configuration's spectral setting
+    (oracle/_ref/libref_k4_fast.so) on the host's cores for the whole
+    frame, and the fixed-RMSE check against that build's FP64 film."""
     import numpy as np
     import torch
+
+    from lambda_b200 import synth
+    from lambda_b200.renderer import Context
+    from lambda_b200.scene import SpectralConfig, flatten, load_nls
+    root = os.path.join(tempfile.gettempdir(), "lgpu_bench", "box")
+    nls = synth.box_room(root, width=BOX["width"])
+    cfg = SpectralConfig(n_bins=81, lambda_inf=380.0, lambda_sup=780.0, hero_k=4)
+    fs = flatten(load_nls(nls, cfg))
+    ctx = Context(device)
+    ctx.upload(fs)
+    W, H = ctx.size
+    spp, B, p = BOX["spp"], BOX["bounces"], BOX["p"]
+    paths = W * H * spp
+    d_out = torch.empty(W * H * 3, dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+    for k in range(warmup):
+        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=100 + k, stream=stream.cuda_stream)
+    total = 0.0
+    for k in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=k, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+    host = np.empty((H, W, 3), np.float32)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        ctx.upload(fs)
+        ctx.render(spp, B, p, seed=k, out=host)
+    e2e_s = time.perf_counter() - t0
+    out = {"value": paths * steps / total / 1e6, "unit": UNIT, "ms_per_frame": total / steps * 1e3,
+           "launches_per_frame": int(ctx.stats()["launches"]),
+           "e2e": {"value": paths * steps / e2e_s / 1e6, "unit": UNIT,
+                   "h2d_bytes_per_step": int(ctx.stats()["upload_bytes"]), "d2h_bytes_per_step": W * H * 12},
+           "workload": BOX_DESC}
+    from oracle import refharness
+    if refharness.available(fast=True, k4=True):
+        ref = refharness.RefScene(nls, fast=True, k4=True)
+        ref.render_rows(spp, B, p, 0, H)
+        reps = 3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            ref.render_rows(spp, B, p, 0, H)
+        v = paths * reps / (time.perf_counter() - t0) / 1e6
+        out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": ref.L.ref_max_threads(), "kind": "reference",
+                               "sample": "the whole frame (%d paths), reference built with 4 hero wavelengths, "
+                                         "81 bins on 380-780 nm" % paths}
+        out["vs_cpu"] = {"value": out["value"] / v, "e2e": out["e2e"]["value"] / v}
+        out["rmse"] = rmse_check(ctx, dict(spp=spp, bounces=B, p=p), nls, d_out, stream, n_rows=H,
+                                 oracle_spp=512, hi_spp=256, k4=True)
+    ctx.close()
+    return out
+
+
+def image_stats(img, oracle):
+    """Relative RMSE per channel against the oracle, and the bias: the mean
+    per-pixel difference over its standard error (pixels draw independent
+    streams) and the ratio of the means with its standard error."""
+    import numpy as np
+    d = (np.asarray(img, np.float64) - oracle).reshape(-1, 3)
+    o = np.asarray(oracle, np.float64).reshape(-1, 3)
+    se = d.std(axis=0, ddof=1) / np.sqrt(d.shape[0])
+    om = o.mean(axis=0)
+    rrmse = np.sqrt(np.mean(d ** 2, axis=0)) / np.sqrt(np.mean(o ** 2, axis=0))
+    return {"rel_rmse": rrmse.tolist(), "t": (d.mean(axis=0) / se).tolist(),
+            "mean_ratio": (1.0 + d.mean(axis=0) / om).tolist(), "mean_ratio_se": (se / om).tolist()}
+
+
+def rmse_check(ctx, w, nls, d_out, stream, n_rows=24, oracle_spp=1024, hi_spp=512, k4=False):
+    """Fixed-RMSE check against the reference itself: on n_rows scene rows
+    spread over the frame, an FP64-film oracle rendered by the reference
+    (oracle/_ref, fast build) at oracle_spp on streams disjoint from its
+    own render (seed base w*h); the reference's own rows at the workload's
+    spp (Renderer::render's streams); the device frame at that spp and at
+    hi_spp.  Reports relative RMSE of both against the oracle, their ratio,
+    and the device's and the reference's mean ratios to the oracle with
+    standard errors."""
+    import numpy as np
+    import torch
+    from oracle import refharness
+    ref = refharness.RefScene(nls, fast=True, k4=k4)
     W, H = ctx.size
     spp, B, p = w["spp"], w["bounces"], w["p"]
-    acc = np.zeros((H, W, 3), np.float64)
-    for k in range(oracle_renders):
-        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=999, spp_offset=k * spp,
-                          stream=stream.cuda_stream)
+    rows = sorted(set(int(round(x)) for x in np.linspace(0, H - 1, n_rows)))
+    t0 = time.perf_counter()
+    orc = np.stack([ref.render_rows(oracle_spp, B, p, r, r + 1, fp64=True, seed_base=W * H)[0] for r in rows])
+    t_orc = time.perf_counter() - t0
+    cref = np.stack([ref.render_rows(spp, B, p, r, r + 1)[0] for r in rows]).astype(np.float64)
+
+    def device_rows(n_spp, seed):
+        ctx.render_device(n_spp, B, p, d_out.data_ptr(), seed=seed, stream=stream.cuda_stream)
         torch.cuda.synchronize()
-        acc += d_out.cpu().numpy().reshape(H, W, 3)
-    oracle = acc / oracle_renders
-    ctx.render_device(spp, B, p, d_out.data_ptr(), seed=1, stream=stream.cuda_stream)
-    torch.cuda.synchronize()
-    gpu = d_out.cpu().numpy().reshape(H, W, 3).astype(np.float64)
-    rows = sorted(ref_rows)
-    # scene row r is image row H - 1 - r
-    o = np.stack([oracle[H - 1 - r] for r in rows])
-    g = np.stack([gpu[H - 1 - r] for r in rows])
-    c = np.stack([ref_rows[r].astype(np.float64) for r in rows])
-    den = np.sqrt(np.mean(o ** 2, axis=(0, 1)))
-    e_g = np.sqrt(np.mean((g - o) ** 2, axis=(0, 1))) / den
-    e_c = np.sqrt(np.mean((c - o) ** 2, axis=(0, 1))) / den
-    # means over the rows: a bias between the estimators would show here
-    mean_ratio = np.mean(c, axis=(0, 1)) / np.mean(o, axis=(0, 1))
-    return {"device": [float(x) for x in e_g], "reference": [float(x) for x in e_c],
-            "ratio": [float(x) for x in e_g / e_c], "rows": len(rows),
-            "reference_mean_over_oracle_mean": [float(x) for x in mean_ratio],
-            "oracle": "device, %d spp (%d renders of %d spp with other random streams, FP64 mean)" %
-                      (oracle_renders * spp, oracle_renders, spp),
-            "what": "relative RMSE per channel (R, G, B) over the reference's sampled rows at %d spp" % spp}
+        img = d_out.cpu().numpy().reshape(H, W, 3).astype(np.float64)
+        return np.stack([img[H - 1 - r] for r in rows])  # scene row r is image row H - 1 - r
+
+    dev = image_stats(device_rows(spp, 1), orc)
+    cpu = image_stats(cref, orc)
+    hi = image_stats(device_rows(hi_spp, 2), orc)
+    return {"device": dev, "reference": cpu,
+            "ratio": [a / b for a, b in zip(dev["rel_rmse"], cpu["rel_rmse"])],
+            "device_%dspp" % hi_spp: {"t": hi["t"], "mean_ratio": hi["mean_ratio"],
+                                       "mean_ratio_se": hi["mean_ratio_se"]},
+            "rows": len(rows), "pixels": len(rows) * W, "oracle_seconds": t_orc,
+            "oracle": "reference FP64 film (oracle/_ref fast build), %d spp, seed base w*h (streams disjoint "
+                      "from Renderer::render's), %d rows spread over the frame" % (oracle_spp, len(rows)),
+            "what": "relative RMSE per channel (R, G, B) at %d spp of the device frame and of the reference's "
+                    "own render, both against the oracle; t = mean per-pixel difference / its standard error"
+                    % spp}
 
 
 def cpu_reference_sample(nls, w, budget_s, fast=True, keep=None):
@@ -620,7 +802,7 @@ def run_device(args, w):
     # end to end through the C ABI with host buffers
     import numpy as np
     host = np.empty((H, W, 3), np.float32)
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -637,7 +819,7 @@ def run_device(args, w):
 
     c = counters[-1]
     launches_per_step = int(c["launches"])
-    roofline = kernel_roofline(ctx, spp, B, p, stream)
+    roofline = kernel_roofline(ctx, spp, B, p, stream, clk.get("sm_mhz"))
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -653,14 +835,17 @@ def run_device(args, w):
         line["batched"] = run_batched(Context, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
         line["adjoint"] = run_adjoint(local)
+    if rank == 0 and world == 1 and not args.no_box:
+        line["box_room"] = run_box_room(local)
+    if rank == 0 and world == 1 and not args.no_large:
+        line["large"] = run_large()
     if rank == 0 and world == 1 and not args.no_baseline:
         from oracle import refharness
         if refharness.available(fast=True):
-            rows = {}
-            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s, keep=rows)
+            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
             line["cpu_baseline"] = {"value": v / 1e6, "unit": UNIT, "cores": cores,
                                     "kind": "reference", "sample": sample}
-            line["rmse"] = rmse_check(ctx, w, rows, d_out, stream)
+            line["rmse"] = rmse_check(ctx, w, nls, d_out, stream)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()
@@ -684,7 +869,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-sequential run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint cost and FD check")
     ap.add_argument("--large", action="store_true",
-                    help="the large configuration (4K, 16 tile jobs, one adjoint pass) instead")
+                    help="only the large configuration (4K, 16 tile jobs, one adjoint pass)")
+    ap.add_argument("--no-large", action="store_true", help="skip the large configuration")
+    ap.add_argument("--no-box", action="store_true", help="skip the box-room configuration")
     ap.add_argument("--ref-step-s", type=float, default=8.0,
                     help="seconds of reference CPU work per sampled step")
     args = ap.parse_args()
@@ -696,7 +883,13 @@ def main():
     if args.impl == "reference":
         return run_reference(args, w)
     if args.large:
-        return run_large(args)
+        big = run_large(args.spp)
+        line = {"metric": METRIC, "value": big["value"], "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 1,
+                "ms_per_step": big["seconds"] * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+                "config": {"workload": LARGE_DESC, "paths": big["paths"]}, "large": big}
+        print(json.dumps(line))
+        return 0
     return run_device(args, w)
 
 

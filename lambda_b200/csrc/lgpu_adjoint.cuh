@@ -253,6 +253,8 @@ __global__ void __launch_bounds__(128, 10) wf_shade_adjoint(OneJob jobs, WaveSta
     bool cont = false, scatter = false, visible = false;
     f3 np = f3{0.f, 0.f, 0.f}, nd = f3{0.f, 0.f, 1.f};
     float lis_scale = 0.f, m_scale = 0.f, hero = 0.f;
+    // d ln w_L / dα and d ln w_mat / dα of the MIS weights (below)
+    float dlw_L = 0.f, dlw_mat = 0.f;
     uint64_t rng = 0;
     uint32_t mat = 0, light = 0, depth = 0;
     bool front = true;
@@ -295,10 +297,25 @@ __global__ void __launch_bounds__(128, 10) wf_shade_adjoint(OneJob jobs, WaveSta
           float w_L = 1.f, w_mat = 0.f;
           if (ms.ok) {
             float const p_L_mati = prob_for_light(S, L, H.p, ms.dir) * prob_l;
-            float const p_mat_Li = prob_for_material(S, m, x0, H, ls.dir, o, a.sample_p);
+            float dlp_Li = 0.f;
+            float const p_mat_Li = prob_for_material(S, m, x0, H, ls.dir, o, a.sample_p, &dlp_Li);
             float const p_L_i = ls.prob * prob_l;
             w_L = p_L_i * p_L_i / (p_L_i * p_L_i + p_mat_Li * p_mat_Li);
             w_mat = ms.prob * ms.prob / (ms.prob * ms.prob + p_L_mati * p_L_mati);
+            // The power-heuristic weights depend on α through the material
+            // pdf (at the light sample's direction for w_L, at the material
+            // sample's for w_mat).  In a proper MIS their derivatives would
+            // cancel in expectation; here they do not, because the
+            // reference applies w_L only when a material sample exists
+            // (src/renderer.cpp:120) and w_mat to the whole recursive
+            // radiance (src/renderer.cpp:145), so the gradient of its
+            // expected image carries them:
+            //   d ln w_L / dα   = -2 (1 - w_L) d ln p_mat(ω_L) / dα
+            //   d ln w_mat / dα =  2 (1 - w_mat) d ln p_mat(ω_mat) / dα
+            // (the sample's own 1/pdf needs no term: its α-derivative equals
+            // the score of the density the direction was drawn from).
+            dlw_L = -2.f * (1.f - w_L) * dlp_Li;
+            dlw_mat = 2.f * (1.f - w_mat) * ms.dlnprob;
           }
           lis_scale = ls.scale / (ls.prob * prob_l) * w_L;
           m_scale = ms.ok ? w_mat / ms.prob : 0.f;
@@ -327,11 +344,14 @@ __global__ void __launch_bounds__(128, 10) wf_shade_adjoint(OneJob jobs, WaveSta
         float const coef = bsdf_k(S, m, bl, x, l, front);
         float const rad = spec_at(S, L.spectrum, x);
         grad_bsdf(S, m, mat, bl, x, l, front, gw * b * rad * lis_scale, g, g_d, g_alpha);
-        rem -= b * (rad * coef * lis_scale);
+        float const nee = b * (rad * coef * lis_scale);
+        g_alpha += gw * nee * dlw_L;
+        rem -= nee;
       }
       if (cont) {
         float const f = mat_mult_k(S, m, ms, x, l, front);
         grad_mult(S, m, ms, x, l, f, gw * rem, g, g_d, g_alpha);
+        g_alpha += gw * rem * dlw_mat;
         out.beta[k * cap + o_pos] = b * (f * m_scale);
         out.acc[k * cap + o_pos] = rem;
         out.gw[k * cap + o_pos] = gw;

@@ -414,6 +414,7 @@ struct MatSample {
   float a, b, c;
   float cos_oh;  // blinn: o·h, for the per-wavelength total-internal-reflection test
   float lnhn;    // log of the |cosine| raised to α in c (for d/dα)
+  float dlnprob; // d ln(prob) / dα: 0 for the lobes whose pdf does not depend on α
 };
 
 template <class R>
@@ -423,7 +424,7 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
   ms.ok = false;
   ms.prob = 0.f;
   ms.lobe = 0;
-  ms.a = ms.b = ms.c = ms.cos_oh = ms.lnhn = 0.f;
+  ms.a = ms.b = ms.c = ms.cos_oh = ms.lnhn = ms.dlnprob = 0.f;
   ms.dir = f3{0.f, 0.f, 1.f};
   f3 const n = H.front ? H.F.z : neg3(H.F.z);
   if (m.type == LGPU_MAT_LAMBERTIAN) {  // cg.hpp:1755-1777
@@ -478,6 +479,8 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
       ms.cos_oh = cos_oh;
       ms.c = powf(w.z, m.alpha);
       ms.lnhn = logf(fabsf(w.z));
+      // hp = (α+1)/(2π) |h·n|^(α+1)
+      ms.dlnprob = 1.f / (m.alpha + 1.f) + ms.lnhn;
       if (lobe < pp_spec * p_r) {
         ms.prob = pp_spec * p_r * hp * 0.25f;
         ms.dir = reflect(o, h);
@@ -514,6 +517,7 @@ __device__ __forceinline__ MatSample sample_material(const DevScene& S, const De
     ms.ok = true;
     ms.dir = i;
     ms.prob = p * powf(fdot(nz, h), m.alpha + 1.f) * (m.alpha + 1.f) * 0.5f * kInvPi * 0.25f;
+    ms.dlnprob = 1.f / (m.alpha + 1.f) + logf(fdot(nz, h));
     // its mult is thinfilm::BRDFcosθ(l, i, o, F.z, front)
     ms.lobe = 0;
     if (!(fdot(i, nz) < 0.f) && !(fdot(o, nz) < 0.f)) {
@@ -560,8 +564,12 @@ __device__ __forceinline__ float mat_mult_k(const DevScene& S, const DevMaterial
 // (src/renderer.cpp:136-137): probForBlinn and probForThinFilm declare
 // (o, i) where the call passes (i, o), so inside them `o` is the light
 // direction and `i` the view direction.
+// With dlog, also d ln(prob) / dα (0 where the pdf does not depend on α),
+// for the path-replay adjoint; the returned pdf is the same either way.
 __device__ __forceinline__ float prob_for_material(const DevScene& S, const DevMaterial& m, float x0,
-                                                   const HitInfo& H, f3 wl, f3 o, float p) {
+                                                   const HitInfo& H, f3 wl, f3 o, float p,
+                                                   float* dlog = nullptr) {
+  if (dlog) *dlog = 0.f;
   f3 const n = H.front ? H.F.z : neg3(H.F.z);
   if (m.type == LGPU_MAT_LAMBERTIAN) {  // cg.hpp:1780-1787
     float const ci = fdot(wl, n);
@@ -591,9 +599,15 @@ __device__ __forceinline__ float prob_for_material(const DevScene& S, const DevM
     }
     float const hn = fdot(h, n);
     float const hp = powf(fabsf(hn), m.alpha + 1.f) * (m.alpha + 1.f) * 0.5f * kInvPi;
-    if (refl) return p * (m.p_d * (fabsf(cos_in) * kInvPi) + m.p_spec * p_r * hp * 0.25f);
+    if (refl) {
+      float const spec = m.p_spec * p_r * hp * 0.25f;
+      float const tot_p = p * (m.p_d * (fabsf(cos_in) * kInvPi) + spec);
+      if (dlog && tot_p > 0.f) *dlog = p * spec * (1.f / (m.alpha + 1.f) + logf(fabsf(hn))) / tot_p;
+      return tot_p;
+    }
     float const c2 = 1.f - ior * ior * (1.f - cos_o * cos_o);
     if (c2 < 0.f) return 0.f;
+    if (dlog) *dlog = 1.f / (m.alpha + 1.f) + logf(fabsf(hn));
     return p * m.p_spec * p_t * hp * 0.25f;
   }
   if (m.type == LGPU_MAT_THINFILM) {  // cg.hpp:1932-1949 with o := wl, i := o
@@ -601,6 +615,7 @@ __device__ __forceinline__ float prob_for_material(const DevScene& S, const DevM
     f3 const bo = wl, bi = o;
     if (!H.front || fdot(bi, nz) < 0.f || fdot(bo, nz) < 0.f) return 0.f;
     f3 const h = half_vec(bi, bo, nz);
+    if (dlog) *dlog = 1.f / (m.alpha + 1.f) + logf(fdot(bo, h));
     return p * powf(fdot(bo, h), m.alpha + 1.f) * (m.alpha + 1.f) * 0.5f * kInvPi * 0.25f;
   }
   return 0.f;

@@ -14,9 +14,11 @@ stores:
     REF_SPP samples per pixel (float film, as the reference renders);
   * the same rows as an FP64-accumulated ORACLE_SPP-sample oracle drawn
     from streams disjoint from the reference's render (seed base w*h);
-  * the median over MSE_RENDERS independent reference renders of those rows
-    at REF_SPP (seed bases 2*w*h, 3*w*h, ...) of their relative MSE against
-    the stored oracle, per channel.
+  * the error statistics of MSE_RENDERS independent reference renders of
+    those rows at REF_SPP (seed bases 2*w*h, 3*w*h, ...) against the stored
+    oracle, per channel: the median and 90th percentile of |img - oracle| /
+    RMS(oracle) pooled over the renders' pixels, and the median of their
+    relative MSEs.
 The GPU test (tests/test_gpu_render.py) rebuilds the scene from the arrays,
 renders it on the device and compares against these rows.
 """
@@ -60,11 +62,13 @@ def generate():
     img_orc = np.stack([ref.render_rows(ORACLE_SPP, BOUNCES, SAMPLE_P, r, r + 1, fp64=True,
                                         seed_base=W * H)[0] for r in rows])
     orc = img_orc.astype(np.float32).astype(np.float64)
-    mses = []
+    scale = np.sqrt(np.mean(orc ** 2, axis=(0, 1)))
+    mses, errs = [], []
     for k in range(MSE_RENDERS):
         img = np.stack([ref.render_rows(REF_SPP, BOUNCES, SAMPLE_P, r, r + 1, seed_base=(2 + k) * W * H)[0]
                         for r in rows]).astype(np.float64)
         mses.append(np.sum((img - orc) ** 2, axis=(0, 1)) / np.sum(orc ** 2, axis=(0, 1)))
+        errs.append((np.abs(img - orc) / scale).reshape(-1, 3))
     np.savez_compressed(
         PATH, camera=_raw(ctypes.addressof(sc.cam), 1, L.Camera),
         spec=np.array([nb, sc.spec.hero_k], np.uint32),
@@ -75,7 +79,8 @@ def generate():
         spectra=np.ctypeslib.as_array(sc.spectra, (sc.n_spectra * nb,)).astype(np.float32),
         rows=rows, ref=img_ref.astype(np.float32), oracle=img_orc.astype(np.float32),
         settings=np.array([REF_SPP, ORACLE_SPP, BOUNCES], np.int64),
-        ref_mse_median=np.median(mses, axis=0), ref_mse_renders=np.array([MSE_RENDERS], np.int64),
+        ref_mse_median=np.median(mses, axis=0), ref_renders=np.array([MSE_RENDERS], np.int64),
+        ref_err_quantiles=np.percentile(np.concatenate(errs), [50, 90], axis=0),
         sample_p=np.array([SAMPLE_P], np.float32))
     return PATH
 
