@@ -302,6 +302,22 @@ def run_batched(ctx_cls, device, n_jobs=64):
     t_b = timed(batched)
     t_s = timed(sequential)
     equal = all(torch.equal(a, b) for a, b in zip(outs, seq))
+    # each job alone, timed: the best rate any job reaches alone is the
+    # steady state of the wavefront on these scenes; batching can at best
+    # run every path at that rate, so total paths / that rate bounds the
+    # batched time from below and t_s / it the speedup from above
+    job_paths = [j["width"] * j["width"] * j["spp"] for j in specs]
+    job_s = [timed(lambda j=j, o=o: ctx.render_batch_device([j], [o.data_ptr()], stream=stream.cuda_stream))
+             for j, o in zip(jobs, seq)]
+    best_rate = max(pth / t for pth, t in zip(job_paths, job_s))
+    bound = t_s / (paths / best_rate)
+    # the small jobs (at most 256x256 pixels and 16 spp): batched vs back to back
+    small = [k for k, j in enumerate(specs) if j["width"] <= 256 and j["spp"] <= 16]
+    small_paths = sum(job_paths[k] for k in small)
+    t_bs = timed(lambda: ctx.render_batch_device([jobs[k] for k in small], [ptrs[k] for k in small],
+                                                 stream=stream.cuda_stream)) if small else 0.0
+    t_ss = timed(lambda: [ctx.render_batch_device([jobs[k]], [seq[k].data_ptr()], stream=stream.cuda_stream)
+                          for k in small]) if small else 0.0
     # the library's autotuner on the same jobs at spp / 16, then the batch
     # again with the launch shape it chose
     t0 = time.perf_counter()
@@ -311,7 +327,15 @@ def run_batched(ctx_cls, device, n_jobs=64):
     t_t = timed(batched)
     equal_t = all(torch.equal(a, b) for a, b in zip(outs, seq)) if not cfg["mega_items"] else None
     return {"value": paths / t_t / 1e6, "unit": UNIT, "sequential_value": paths / t_s / 1e6,
-            "speedup": t_s / t_t, "batched_default_value": paths / t_b / 1e6,
+            "speedup": t_s / t_t, "speedup_bound": bound,
+            "bound": "sequential time / (total paths / the best rate of any job rendered alone, %.1f Mpaths/s): "
+                     "what batching could gain if every path ran at the steady-state rate" % (best_rate / 1e6),
+            "small_jobs": {"jobs": len(small), "paths": small_paths,
+                           "batched_value": small_paths / t_bs / 1e6 if t_bs else None,
+                           "sequential_value": small_paths / t_ss / 1e6 if t_ss else None,
+                           "speedup": t_ss / t_bs if t_bs else None,
+                           "what": "the jobs of at most 256x256 pixels and 16 spp, batched vs back to back"},
+            "batched_default_value": paths / t_b / 1e6,
             "speedup_default_config": t_s / t_b, "batched_s": t_t, "batched_default_s": t_b,
             "sequential_s": t_s, "paths": paths, "jobs": n_jobs, "images_identical": bool(equal),
             "images_identical_tuned": equal_t, "autotune": {"config": cfg, "seconds": tune_s},
@@ -577,8 +601,21 @@ def run_box_room(device, steps=20, warmup=3):
         ctx.upload(fs)
         ctx.render(spp, B, p, seed=k, out=host)
     e2e_s = time.perf_counter() - t0
+    launches = int(ctx.stats()["launches"])
+    # the one-thread-per-pixel megakernel on the same frame (same paths)
+    from lambda_b200 import _lib as L
+    mega = 0.0
+    for k in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.render_device(spp, B, p, d_out.data_ptr(), seed=k, flags=L.FLAG_MEGAKERNEL, stream=stream.cuda_stream)
+        e1.record(stream)
+        e1.synchronize()
+        mega += e0.elapsed_time(e1) / 1e3
     out = {"value": paths * steps / total / 1e6, "unit": UNIT, "ms_per_frame": total / steps * 1e3,
-           "launches_per_frame": int(ctx.stats()["launches"]),
+           "launches_per_frame": launches, "megakernel_value": paths * steps / mega / 1e6,
            "e2e": {"value": paths * steps / e2e_s / 1e6, "unit": UNIT,
                    "h2d_bytes_per_step": int(ctx.stats()["upload_bytes"]), "d2h_bytes_per_step": W * H * 12},
            "workload": BOX_DESC}
@@ -831,6 +868,15 @@ def run_device(args, w):
             "e2e": e2e, "roofline": roofline, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
+    if rank == 0 and world == 1 and not args.no_baseline:
+        # the reference's pixel loop on the host's cores, before the sections
+        # below load those cores with oracle renders
+        from oracle import refharness
+        if refharness.available(fast=True):
+            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
+            line["cpu_baseline"] = {"value": v / 1e6, "unit": UNIT, "cores": cores,
+                                    "kind": "reference", "sample": sample}
+            line["rmse"] = rmse_check(ctx, w, nls, d_out, stream)
     if rank == 0 and world == 1 and not args.no_batch:
         line["batched"] = run_batched(Context, local)
     if rank == 0 and world == 1 and not args.no_adjoint:
@@ -839,13 +885,6 @@ def run_device(args, w):
         line["box_room"] = run_box_room(local)
     if rank == 0 and world == 1 and not args.no_large:
         line["large"] = run_large()
-    if rank == 0 and world == 1 and not args.no_baseline:
-        from oracle import refharness
-        if refharness.available(fast=True):
-            v, cores, sample = cpu_reference_sample(nls, w, args.ref_step_s)
-            line["cpu_baseline"] = {"value": v / 1e6, "unit": UNIT, "cores": cores,
-                                    "kind": "reference", "sample": sample}
-            line["rmse"] = rmse_check(ctx, w, nls, d_out, stream)
     if rank == 0:
         print(json.dumps(line))
     ctx.close()

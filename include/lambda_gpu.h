@@ -35,9 +35,10 @@ extern "C" {
 
 /* 2: lgpu_stats gained order_rays; lgpu_probe_shading and
    lgpu_build_bvh_device were added.
-   3: lgpu_stats gained local_stack; lgpu_trace_any and
-   LGPU_FLAG_FP64_FILM were added; lgpu_trace_closest runs the render's
-   traversal kernels */
+   3: lgpu_stats gained local_stack; lgpu_trace_any,
+   LGPU_FLAG_FP64_FILM and lgpu_scene.flags (LGPU_SCENE_HOST_LAYOUT) were
+   added; lgpu_trace_closest runs the render's traversal kernels; uploads
+   lay the meshes out on the device */
 #define LGPU_ABI_VERSION 3
 
 typedef struct lgpu_ctx lgpu_ctx;
@@ -172,10 +173,18 @@ typedef struct lgpu_mesh {
   const uint32_t* prim_idxs;
 } lgpu_mesh;
 
+/* lgpu_scene.flags: lay the meshes out on the host (the relayout pass of
+   lgpu_upload_scene run on the CPU) instead of on the device.  The device
+   reads the meshes' own arrays (V, N, GN, F and the BVH) and builds their
+   nodes, leaf triangles and shading records itself; both give identical
+   device data. */
+#define LGPU_SCENE_HOST_LAYOUT 0x1u
+
 typedef struct lgpu_scene {
   lgpu_camera cam;
   lgpu_spectral spec;
-  uint32_t n_objects, n_materials, n_lights, n_meshes, n_spectra, reserved;
+  uint32_t n_objects, n_materials, n_lights, n_meshes, n_spectra;
+  uint32_t flags; /* LGPU_SCENE_* upload options (0: defaults) */
   const lgpu_object* objects;
   const lgpu_material* materials;
   const lgpu_light* lights;

@@ -86,7 +86,7 @@ class Scene(ctypes.Structure):
     _fields_ = [("cam", Camera), ("spec", Spectral),
                 ("n_objects", ctypes.c_uint32), ("n_materials", ctypes.c_uint32),
                 ("n_lights", ctypes.c_uint32), ("n_meshes", ctypes.c_uint32),
-                ("n_spectra", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("n_spectra", ctypes.c_uint32), ("flags", ctypes.c_uint32),
                 ("objects", ctypes.POINTER(Object)), ("materials", ctypes.POINTER(Material)),
                 ("lights", ctypes.POINTER(Light)), ("meshes", ctypes.POINTER(Mesh)),
                 ("spectra", c_float_p)]
@@ -143,6 +143,8 @@ class Stats(ctypes.Structure):
 
 FLAG_KERNEL_TIMING = 0x4
 FLAG_FP64_FILM = 0x8
+# lgpu_scene.flags
+SCENE_HOST_LAYOUT = 0x1
 KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2
 
 

@@ -11,6 +11,7 @@
 #include "lambda_gpu.h"
 #include "lgpu_kernels.cuh"
 #include "lgpu_layout.h"
+#include "lgpu_layout_dev.h"
 
 using namespace lgpu;
 
@@ -71,6 +72,11 @@ struct lgpu_ctx {
   // the scene table (lgpu_upload_scenes); S is a copy of slot 0's DevScene
   std::vector<SceneSlot> slots;
   HostLayout layout;  // host side of the last upload (its arrays are reused)
+  // meshes laid out on the device (lgpu_layout_dev.cu): what to build, the
+  // raw arrays of one mesh at a time, and the kernels' error word
+  DeviceLayoutWork dev_layout;
+  DevArray<uint8_t> raw;
+  DevArray<uint32_t> layout_err;
   // batch tables (lgpu_render_batch)
   DevArray<DevJob> jobs;
   DevArray<uint64_t> job_items;
@@ -563,17 +569,95 @@ bool timing_requested(const lgpu_render_params* p) {
 }
 
 // Lays out one scene on the host and copies it into a scene slot.
+// The raw arrays of the meshes of the last device-layout upload, one mesh
+// at a time through ctx->raw (256-byte aligned pieces), and the kernels
+// that lay them out into the slot's node, triangle and shading arrays.
+int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene, uint64_t& bytes) {
+  const DeviceLayoutWork& W = ctx->dev_layout;
+  cudaStream_t const st = ctx->stream;
+  auto pieces = [](const lgpu_mesh& m, size_t (&sz)[8]) {
+    sz[0] = 12 * size_t(m.n_positions);
+    sz[1] = 12 * size_t(m.n_normals);
+    sz[2] = 12 * size_t(m.n_faces);
+    sz[3] = 4 * size_t(m.f_stride) * m.n_faces;
+    sz[4] = 8 * size_t(m.n_nodes);
+    sz[5] = 192 * size_t(m.n_bbs);
+    sz[6] = 4 * size_t(m.n_prim_idxs);
+    sz[7] = 4 * size_t(m.n_nodes);
+    size_t t = 0;
+    for (size_t x : sz) t += (x + 255) & ~size_t(255);
+    return t;
+  };
+  size_t most = 0;
+  for (const DeviceMeshJob& j : W.jobs) {
+    size_t sz[8];
+    most = std::max(most, pieces(scene.meshes[j.mesh], sz));
+  }
+  cudaError_t e = ensure(ctx->raw, most);
+  if (e == cudaSuccess) e = ensure(ctx->layout_err, 1);
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->layout_err.ptr, 0xFF, sizeof(uint32_t), st);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "mesh layout buffers");
+  for (const DeviceMeshJob& j : W.jobs) {
+    const lgpu_mesh& m = scene.meshes[j.mesh];
+    size_t sz[8];
+    pieces(m, sz);
+    const void* src[8] = {m.V, m.N, m.GN, m.F, m.nodes, m.bbs, m.prim_idxs, W.childref.data() + j.childref_off};
+    void* dst[8];
+    size_t off = 0;
+    for (int k = 0; k < 8 && e == cudaSuccess; k++) {
+      dst[k] = ctx->raw.ptr + off;
+      off += (sz[k] + 255) & ~size_t(255);
+      if (sz[k]) e = cudaMemcpyAsync(dst[k], src[k], sz[k], cudaMemcpyHostToDevice, st);
+      bytes += sz[k];
+    }
+    MeshRaw const r{static_cast<const float*>(dst[0]), static_cast<const float*>(dst[1]),
+                    static_cast<const float*>(dst[2]), static_cast<const uint32_t*>(dst[3]),
+                    static_cast<const uint32_t*>(dst[4]), static_cast<const float*>(dst[5]),
+                    static_cast<const uint32_t*>(dst[6]), static_cast<const uint32_t*>(dst[7]),
+                    m.n_positions, m.n_normals, m.n_faces, m.f_stride, m.n_nodes, m.n_prim_idxs};
+    if (e == cudaSuccess)
+      e = build_mesh_layout(r, j.mesh, sl.nodes.ptr, sl.tris.ptr + j.slot_base, sl.shade.ptr + j.face_base,
+                            ctx->layout_err.ptr, st);
+    // the next mesh's copies reuse ctx->raw: stream order puts them after
+    // these kernels; the host's pageable copies return once staged
+  }
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "mesh layout");
+  return LGPU_OK;
+}
+
 int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
   HostLayout& L = ctx->layout;
   std::string err;
-  int const rc = make_layout(scene, L, err);
+  bool const on_device = !(scene.flags & LGPU_SCENE_HOST_LAYOUT);
+  DeviceLayoutWork& W = ctx->dev_layout;
+  int const rc = make_layout(scene, L, err, on_device ? &W : nullptr);
   if (rc != LGPU_OK) return fail(ctx, rc, err);
   cudaStream_t const st = ctx->stream;
+  uint64_t bytes = 0;
   cudaError_t e = upload(sl.objects, L.objects, st);
   if (e == cudaSuccess) e = upload(sl.meshes, L.meshes, st);
-  if (e == cudaSuccess) e = upload(sl.nodes, L.nodes, st);
-  if (e == cudaSuccess) e = upload(sl.tris, L.tris, st);
-  if (e == cudaSuccess) e = upload(sl.shade, L.shade, st);
+  if (on_device) {
+    // the meshes' nodes first (built on the device), then the instance BVH's
+    size_t const n_nodes = size_t(W.mesh_nodes) + L.nodes.size();
+    if (e == cudaSuccess) e = ensure(sl.nodes, n_nodes);
+    if (e == cudaSuccess) e = ensure(sl.tris, W.mesh_slots);
+    if (e == cudaSuccess) e = ensure(sl.shade, W.mesh_faces);
+    sl.nodes.n = n_nodes;
+    sl.tris.n = W.mesh_slots;
+    sl.shade.n = W.mesh_faces;
+    if (e == cudaSuccess && !L.nodes.empty())
+      e = cudaMemcpyAsync(sl.nodes.ptr + W.mesh_nodes, L.nodes.data(), L.nodes.size() * sizeof(WideNode),
+                          cudaMemcpyHostToDevice, st);
+    bytes += L.nodes.size() * sizeof(WideNode);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scene upload");
+    if (int r = build_meshes_on_device(ctx, sl, scene, bytes)) return r;
+  } else {
+    if (e == cudaSuccess) e = upload(sl.nodes, L.nodes, st);
+    if (e == cudaSuccess) e = upload(sl.tris, L.tris, st);
+    if (e == cudaSuccess) e = upload(sl.shade, L.shade, st);
+    bytes += L.nodes.size() * sizeof(WideNode) + L.tris.size() * sizeof(TriSlot) +
+             L.shade.size() * sizeof(FaceShade);
+  }
   if (e == cudaSuccess) e = upload(sl.spectra, L.spectra, st);
   if (e == cudaSuccess) e = upload(sl.mats, L.mats, st);
   if (e == cudaSuccess) e = upload(sl.lights, L.lights, st);
@@ -581,6 +665,21 @@ int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
   if (e == cudaSuccess) e = upload(sl.cmf, L.cmf, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "scene upload");
+  if (on_device) {
+    uint32_t code = UINT32_MAX;
+    e = cudaMemcpy(&code, ctx->layout_err.ptr, sizeof(code), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "scene upload");
+    if (code != UINT32_MAX) {
+      uint32_t const mi = code / 4;
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT,
+                  (code % 4 == 1 ? "face index out of range in mesh " : "BVH primitive index out of range in mesh ") +
+                      std::to_string(mi));
+    }
+  }
+  bytes += L.objects.size() * sizeof(DevObject) + L.meshes.size() * sizeof(DevMesh) +
+           L.spectra.size() * sizeof(float) + L.mats.size() * sizeof(DevMaterial) +
+           L.lights.size() * sizeof(lgpu_light) + L.tlas_objects.size() * sizeof(uint32_t) +
+           L.cmf.size() * sizeof(float);
   DevScene& S = sl.S;
   S = DevScene{};
   S.objects = sl.objects.ptr;
@@ -609,11 +708,7 @@ int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
   S.cam = scene.cam;
   std::memcpy(S.tlas_bounds, L.tlas_bounds, sizeof(S.tlas_bounds));
   if (L.max_stack > ctx->stats.max_stack) ctx->stats.max_stack = L.max_stack;
-  sl.bytes = L.objects.size() * sizeof(DevObject) + L.meshes.size() * sizeof(DevMesh) +
-             L.nodes.size() * sizeof(WideNode) + L.tris.size() * sizeof(TriSlot) +
-             L.shade.size() * sizeof(FaceShade) + L.spectra.size() * sizeof(float) +
-             L.mats.size() * sizeof(DevMaterial) + L.lights.size() * sizeof(lgpu_light) +
-             L.tlas_objects.size() * sizeof(uint32_t) + L.cmf.size() * sizeof(float);
+  sl.bytes = bytes;
   return LGPU_OK;
 }
 
@@ -664,6 +759,12 @@ void lgpu_destroy(lgpu_ctx* ctx) {
   if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   ctx->rays.release();
   ctx->hits.release();
+  ctx->trace_arena.release();
+  ctx->trace_tmax.release();
+  ctx->trace_skip.release();
+  ctx->trace_any.release();
+  ctx->raw.release();
+  ctx->layout_err.release();
   ctx->probes.release();
   ctx->probe_out.release();
   ctx->partials.release();

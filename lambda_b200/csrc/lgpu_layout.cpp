@@ -220,83 +220,45 @@ void parallel_for(size_t n, F fn) {
   for (auto& t : ts) t.join();
 }
 
-// Re-lays a reference-format wide BVH into WideNodes appended to `nodes`.
-// Leaf children point at slot_base + (first primitive position).  Returns
-// the root reference through root_ref and the stack bound through max_stack.
-bool relayout(const RefView& R, uint32_t slot_base, BigVector<WideNode>& nodes, uint32_t& root_ref,
-              uint32_t& max_stack, std::string& err) {
+// The first pass of the relayout of a reference-format wide BVH: validates
+// its nodes and gives every reference node q its child reference
+// childref[q] (interior: node_base + its rank among the interior nodes;
+// leaf: kLeafBit | (count-1) << 28 | slot_base + first primitive
+// position).  Returns the number of interior nodes, the root reference and
+// the stack bound.
+bool relayout_meta(const RefView& R, uint32_t node_base, uint32_t slot_base, uint32_t* childref,
+                   uint32_t& n_int_out, uint32_t& root_ref, uint32_t& max_stack, std::string& err) {
   if (R.n_nodes == 0) {
     err = "BVH has no nodes";
     return false;
   }
-  uint32_t const node_base = uint32_t(nodes.size());
-  std::vector<uint32_t> wide(R.n_nodes, 0xFFFFFFFFu);
   uint32_t n_int = 0;
-  for (uint32_t r = 0; r < R.n_nodes; r++)
-    if (!ref_leaf(R.nodes[2 * size_t(r) + 1])) wide[r] = node_base + n_int++;
+  for (uint32_t q = 0; q < R.n_nodes; q++) {
+    uint32_t const d = R.nodes[2 * size_t(q) + 1];
+    if (!ref_leaf(d)) {
+      uint32_t const bbi = R.nodes[2 * size_t(q)];
+      uint32_t const first = ref_idx(d), cnt = ref_count(d);
+      if (bbi >= R.n_bbs || size_t(first) + cnt > R.n_nodes || first <= q) {
+        err = "malformed BVH node";
+        return false;
+      }
+      childref[q] = node_base + n_int++;
+      continue;
+    }
+    uint32_t const start = ref_idx(d), cnt = ref_count(d);
+    if (size_t(start) + cnt > R.n_prims) {
+      err = "BVH leaf primitive range out of bounds";
+      return false;
+    }
+    if (size_t(slot_base) + start + cnt > size_t(kMaxSlots)) {
+      err = "too many leaf primitives for the device layout";
+      return false;
+    }
+    childref[q] = kLeafBit | ((cnt - 1) << 28) | (slot_base + start);
+  }
   if (size_t(node_base) + n_int >= size_t(kLeafBit)) {
     err = "too many BVH nodes";
     return false;
-  }
-  enum { kOk = 0, kLeafRange = 1, kSlots = 2, kMalformed = 3 };
-  // the child reference of node q (0 or an error code)
-  auto ref_of = [&](uint32_t q, uint32_t& out) -> int {
-    uint32_t const d = R.nodes[2 * size_t(q) + 1];
-    if (!ref_leaf(d)) {
-      out = wide[q];
-      return kOk;
-    }
-    uint32_t const start = ref_idx(d), cnt = ref_count(d);
-    if (size_t(start) + cnt > R.n_prims) return kLeafRange;
-    if (size_t(slot_base) + start + cnt > size_t(kMaxSlots)) return kSlots;
-    out = kLeafBit | ((cnt - 1) << 28) | (slot_base + start);
-    return kOk;
-  };
-  nodes.resize(size_t(node_base) + n_int);
-  // every interior node's WideNode, independently of the others
-  std::atomic<int> bad{kOk};
-  parallel_for(R.n_nodes, [&](size_t r0, size_t r1) {
-    for (size_t r = r0; r < r1; r++) {
-      uint32_t const d = R.nodes[2 * r + 1];
-      if (ref_leaf(d)) continue;
-      uint32_t const bbi = R.nodes[2 * r];
-      uint32_t const first = ref_idx(d), cnt = ref_count(d);
-      if (bbi >= R.n_bbs || size_t(first) + cnt > R.n_nodes || first <= r) {
-        bad = kMalformed;
-        return;
-      }
-      const float* bb = R.bbs + 48 * size_t(bbi);
-      WideNode& wn = nodes[wide[r]];
-      for (int c = 0; c < 8; c++) {
-        if (uint32_t(c) < cnt) {
-          wn.lox[c] = bb[0 * 8 + c];
-          wn.loy[c] = bb[1 * 8 + c];
-          wn.loz[c] = bb[2 * 8 + c];
-          wn.hix[c] = bb[3 * 8 + c];
-          wn.hiy[c] = bb[4 * 8 + c];
-          wn.hiz[c] = bb[5 * 8 + c];
-          if (int const e = ref_of(first + c, wn.child[c])) {
-            bad = e;
-            return;
-          }
-        } else {
-          wn.lox[c] = wn.loy[c] = wn.loz[c] = 1e30f;
-          wn.hix[c] = wn.hiy[c] = wn.hiz[c] = -1e30f;
-          wn.child[c] = kEmptyChild;
-        }
-      }
-    }
-  });
-  switch (bad.load()) {
-    case kLeafRange:
-      err = "BVH leaf primitive range out of bounds";
-      return false;
-    case kSlots:
-      err = "too many leaf primitives for the device layout";
-      return false;
-    case kMalformed:
-      err = "malformed BVH node";
-      return false;
   }
   // entries the DFS stack can hold below each node (all children pushed),
   // children first: breadth-first indices grow downwards
@@ -309,11 +271,55 @@ bool relayout(const RefView& R, uint32_t slot_base, BigVector<WideNode>& nodes, 
     for (uint32_t c = 0; c < cnt; c++) deepest = std::max(deepest, bound[first + c]);
     bound[r] = (cnt - 1) + deepest;
   }
-  if (int const e = ref_of(0, root_ref)) {
-    err = e == kLeafRange ? "BVH leaf primitive range out of bounds" : "too many leaf primitives for the device layout";
-    return false;
-  }
+  n_int_out = n_int;
+  root_ref = childref[0];
   max_stack = 1 + bound[0];
+  return true;
+}
+
+// The second pass on the host: the WideNode of every interior node, from
+// its record of child boxes and its children's references (the device
+// builds the same nodes with lgpu::build_mesh_layout).
+void relayout_fill(const RefView& R, const uint32_t* childref, uint32_t node_base, WideNode* nodes) {
+  parallel_for(R.n_nodes, [&](size_t r0, size_t r1) {
+    for (size_t r = r0; r < r1; r++) {
+      uint32_t const d = R.nodes[2 * r + 1];
+      if (ref_leaf(d)) continue;
+      const float* bb = R.bbs + 48 * size_t(R.nodes[2 * r]);
+      uint32_t const first = ref_idx(d), cnt = ref_count(d);
+      WideNode& wn = nodes[childref[r] - node_base];
+      for (int c = 0; c < 8; c++) {
+        if (uint32_t(c) < cnt) {
+          wn.lox[c] = bb[0 * 8 + c];
+          wn.loy[c] = bb[1 * 8 + c];
+          wn.loz[c] = bb[2 * 8 + c];
+          wn.hix[c] = bb[3 * 8 + c];
+          wn.hiy[c] = bb[4 * 8 + c];
+          wn.hiz[c] = bb[5 * 8 + c];
+          wn.child[c] = childref[first + c];
+        } else {
+          wn.lox[c] = wn.loy[c] = wn.loz[c] = 1e30f;
+          wn.hix[c] = wn.hiy[c] = wn.hiz[c] = -1e30f;
+          wn.child[c] = kEmptyChild;
+        }
+      }
+    }
+  });
+}
+
+// Re-lays a reference-format wide BVH into WideNodes appended to `nodes`
+// (node indices continue from node_base, the index of nodes[0]).  Leaf
+// children point at slot_base + (first primitive position).  Returns the
+// root reference through root_ref and the stack bound through max_stack.
+bool relayout(const RefView& R, uint32_t node_base, uint32_t slot_base, BigVector<WideNode>& nodes,
+              uint32_t& root_ref, uint32_t& max_stack, std::string& err) {
+  std::vector<uint32_t> childref(R.n_nodes);
+  uint32_t n_int = 0;
+  uint32_t const first = node_base + uint32_t(nodes.size());
+  if (!relayout_meta(R, first, slot_base, childref.data(), n_int, root_ref, max_stack, err)) return false;
+  size_t const at = nodes.size();
+  nodes.resize(at + n_int);
+  relayout_fill(R, childref.data(), first, nodes.data() + at);
   return true;
 }
 
@@ -359,7 +365,12 @@ int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::st
   return LGPU_OK;
 }
 
-int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
+int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev) {
+  if (dev) {
+    dev->jobs.clear();
+    dev->childref.clear();
+    dev->mesh_nodes = dev->mesh_slots = dev->mesh_faces = 0;
+  }
   // empty every array but keep its capacity
   L.objects.clear();
   L.meshes.clear();
@@ -430,6 +441,42 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       err = "incomplete mesh " + std::to_string(mi);
       return LGPU_ERR_INVALID_ARGUMENT;
     }
+    DevMesh dm{};
+    dm.n_faces = m.n_faces;
+    std::memcpy(dm.bounds, m.bounds, sizeof(dm.bounds));
+    RefView const R{m.n_nodes, m.n_bbs, m.n_prim_idxs, m.nodes, m.bbs, m.prim_idxs};
+    if (dev) {
+      // the device builds this mesh's nodes, leaf triangles and shading
+      // normals (and checks its face and primitive indices) from its raw
+      // arrays; here only the child references and the stack bound
+      DeviceMeshJob j{};
+      j.mesh = mi;
+      j.node_base = dev->mesh_nodes;
+      j.slot_base = dev->mesh_slots;
+      j.face_base = dev->mesh_faces;
+      j.childref_off = dev->childref.size();
+      dev->childref.resize(j.childref_off + m.n_nodes);
+      if (!relayout_meta(R, j.node_base, j.slot_base, dev->childref.data() + j.childref_off, j.n_int, dm.root,
+                         dm.max_stack, err)) {
+        err = "mesh " + std::to_string(mi) + ": " + err;
+        return LGPU_ERR_INVALID_ARGUMENT;
+      }
+      if (dm.max_stack > uint32_t(kStackCap)) {
+        err = "mesh " + std::to_string(mi) + " BVH can need " + std::to_string(dm.max_stack) +
+              " stack entries; the traversal holds " + std::to_string(kStackCap);
+        return LGPU_ERR_UNSUPPORTED;
+      }
+      dm.node_base = j.node_base;
+      dm.slot_base = j.slot_base;
+      dm.face_base = j.face_base;
+      dev->mesh_nodes += j.n_int;
+      dev->mesh_slots += m.n_prim_idxs;
+      dev->mesh_faces += m.n_faces;
+      dev->jobs.push_back(j);
+      L.max_stack = std::max(L.max_stack, dm.max_stack);
+      L.meshes.push_back(dm);
+      continue;
+    }
     std::atomic<bool> bad_face{false}, bad_prim{false};
     parallel_for(m.n_faces, [&](size_t f0, size_t f1) {
       for (size_t f = f0; f < f1; f++) {
@@ -450,14 +497,10 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
       err = "BVH primitive index out of range in mesh " + std::to_string(mi);
       return LGPU_ERR_INVALID_ARGUMENT;
     }
-    DevMesh dm{};
     dm.slot_base = uint32_t(L.tris.size());
     dm.face_base = uint32_t(L.shade.size());
     dm.node_base = uint32_t(L.nodes.size());
-    dm.n_faces = m.n_faces;
-    std::memcpy(dm.bounds, m.bounds, sizeof(dm.bounds));
-    RefView const R{m.n_nodes, m.n_bbs, m.n_prim_idxs, m.nodes, m.bbs, m.prim_idxs};
-    if (!relayout(R, dm.slot_base, L.nodes, dm.root, dm.max_stack, err)) {
+    if (!relayout(R, 0, dm.slot_base, L.nodes, dm.root, dm.max_stack, err)) {
       err = "mesh " + std::to_string(mi) + ": " + err;
       return LGPU_ERR_INVALID_ARGUMENT;
     }
@@ -565,7 +608,8 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err) {
     L.tlas_objects = tl.prim_idxs;
     RefView const R{tl.n_nodes, uint32_t(tl.bbs.size() / 48), uint32_t(tl.prim_idxs.size()),
                     tl.nodes.data(), tl.bbs.data(), tl.prim_idxs.data()};
-    if (!relayout(R, 0, L.nodes, L.tlas_root, L.tlas_max_stack, err)) {
+    // after the meshes' nodes, wherever those are built
+    if (!relayout(R, dev ? dev->mesh_nodes : 0, 0, L.nodes, L.tlas_root, L.tlas_max_stack, err)) {
       err = "instance BVH: " + err;
       return LGPU_ERR_INVALID_ARGUMENT;
     }

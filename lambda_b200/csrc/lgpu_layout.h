@@ -88,9 +88,29 @@ struct HostLayout {
   float tlas_bounds[6] = {0, 0, 0, 0, 0, 0};
 };
 
+// A mesh whose WideNodes, leaf triangles and shading normals are built on
+// the device (build_mesh_layout) from its raw arrays.
+struct DeviceMeshJob {
+  uint32_t mesh;                  // index in the scene
+  uint32_t node_base, n_int;      // its first WideNode and their number
+  uint32_t slot_base, face_base;  // its first TriSlot and FaceShade
+  size_t childref_off;            // its child references in DeviceLayoutWork::childref
+};
+struct DeviceLayoutWork {
+  std::vector<DeviceMeshJob> jobs;
+  // per reference node of each mesh: its child reference (WideNode index,
+  // or leaf: kLeafBit | (count-1) << 28 | first slot)
+  std::vector<uint32_t> childref;
+  uint32_t mesh_nodes = 0, mesh_slots = 0, mesh_faces = 0;  // totals over the meshes
+};
+
 // Validates the scene and lays it out for the device.  Returns LGPU_OK or
-// an lgpu_status with a message in err.
-int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err);
+// an lgpu_status with a message in err.  With dev, the meshes are left to
+// the device: L.nodes then holds only the instance BVH (its node indices
+// follow the meshes' dev->mesh_nodes nodes), L.tris and L.shade stay
+// empty, and dev lists what build_mesh_layout has to build; the face and
+// primitive indices are checked there.
+int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev = nullptr);
 
 // The validated material table alone (for lgpu_update_materials).
 int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::string& err);

@@ -7,6 +7,7 @@ import os
 import numpy as np
 import pytest
 
+from lambda_b200 import _lib as L
 from lambda_b200 import synth
 from lambda_b200.renderer import Context
 from lambda_b200.scene import load_nls
@@ -85,3 +86,65 @@ def test_degenerate_rays(mixed_nls):
     h = ctx.trace(rays)
     assert len(h) == 4
     assert np.all(np.isfinite(h["t"][h["obj"] != 0xFFFFFFFF]))
+
+
+def _upload(ctx, flat, host_layout):
+    flat.scene.flags = L.SCENE_HOST_LAYOUT if host_layout else 0
+    try:
+        return ctx._lib.lgpu_upload_scene(ctx.h, flat.ptr())
+    finally:
+        flat.scene.flags = 0
+
+
+def test_device_layout_equals_host_layout(mixed_nls, scene_dir):
+    """Meshes laid out on the device at upload (the default) and on the host
+    (LGPU_SCENE_HOST_LAYOUT) give bit-identical traces and renders, on the
+    mixed scene and on an instanced scene of several meshes."""
+    import os
+    from lambda_b200 import synth
+    from lambda_b200.scene import FlatScene
+    from tests import raysets
+    inst = synth.instanced(os.path.join(str(scene_dir), "layout_inst"), n_instances=9, subdiv=4, width=48)
+    for nls in (mixed_nls, inst):
+        sc = load_nls(nls)
+        flat = FlatScene(sc)
+        rays = np.concatenate([raysets.camera_rays(sc, 64, seed=1),
+                               raysets.random_rays([-3, -3, 0.01], [3, 3, 3], 20000, seed=2)])
+        out = []
+        for host in (False, True):
+            ctx = Context()
+            assert _upload(ctx, flat, host) == L.OK
+            ctx.flat = flat
+            h = ctx.trace(rays)
+            img = ctx.render(8, 8, 0.8, seed=4)
+            out.append((h, img, ctx.stats()["upload_bytes"]))
+            ctx.close()
+        (h0, i0, b0), (h1, i1, b1) = out
+        assert np.array_equal(h0.view(np.uint8), h1.view(np.uint8))
+        assert np.array_equal(i0.view(np.uint32), i1.view(np.uint32))
+        assert b0 > 0 and b1 > 0
+
+
+def test_device_layout_rejects_bad_indices(mixed_nls):
+    """An out-of-range vertex or BVH primitive index fails the upload with
+    the mesh named, in both layouts, without the device reading it."""
+    from lambda_b200.scene import FlatScene
+    sc = load_nls(mixed_nls)
+    m = next(mm for mm in sc.meshes if mm.F.shape[0] > 4)
+    mi = sc.meshes.index(m)
+    for field, bad, msg in (("F", lambda a: a.__setitem__((3, 1), 10 ** 7), "face index out of range"),
+                            ("prim_idxs", lambda a: a.__setitem__(2, 10 ** 7), "primitive index out of range")):
+        arr = getattr(m, field)
+        saved = arr.copy()
+        bad(arr)
+        try:
+            flat = FlatScene(sc)
+            for host in (False, True):
+                ctx = Context()
+                rc = _upload(ctx, flat, host)
+                assert rc == L.ERR_INVALID_ARGUMENT, (field, host, rc)
+                err = ctx._lib.lgpu_last_error(ctx.h).decode()
+                assert msg in err and ("mesh %d" % mi) in err, err
+                ctx.close()
+        finally:
+            arr[...] = saved
