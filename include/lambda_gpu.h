@@ -158,7 +158,11 @@ typedef struct lgpu_light {
    own layout (cg.hpp:596-631): nodes are {childrenbb_idx, data} pairs with
    data = idx<<4 | (count-1)<<1 | leaf; bbs are aabb_avx2 records of 48
    floats (inf[3][8] then sup[3][8]); prim_idxs index faces.  Position and
-   normal arrays include fast_obj's dummy element at index 0. */
+   normal arrays include fast_obj's dummy element at index 0.
+   A host without the reference's trees passes nodes, bbs and prim_idxs as
+   NULL (counts 0): lgpu_upload_scene then builds the tree as bvh::build
+   does, on the device (lgpu_build_bvh_device; vertex positions must be
+   finite). */
 typedef struct lgpu_mesh {
   uint32_t n_positions, n_normals, n_faces;
   uint32_t f_stride; /* uint32 words per face in F (9 for nl::cg::triangle) */

@@ -77,6 +77,10 @@ struct lgpu_ctx {
   DeviceLayoutWork dev_layout;
   DevArray<uint8_t> raw;
   DevArray<uint32_t> layout_err;
+  // meshes uploaded without a BVH: the trees built for them and the mesh
+  // table pointing at them (build_missing_bvhs)
+  std::vector<RefBvh> built;
+  std::vector<lgpu_mesh> patched;
   // batch tables (lgpu_render_batch)
   DevArray<DevJob> jobs;
   DevArray<uint64_t> job_items;
@@ -625,7 +629,58 @@ int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene
   return LGPU_OK;
 }
 
-int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene) {
+// Meshes passed without their BVH (nodes, bbs and prim_idxs all NULL) get
+// it built here on the device, bit-identical to bvh::build (cg.hpp:632-749);
+// `out` is the scene with those meshes pointing at the built trees, kept in
+// ctx->built until the next upload.
+int build_missing_bvhs(lgpu_ctx* ctx, const lgpu_scene& in, lgpu_scene& out) {
+  out = in;
+  ctx->built.clear();
+  ctx->patched.clear();
+  bool any = false;
+  for (uint32_t mi = 0; mi < in.n_meshes && in.meshes; mi++) {
+    const lgpu_mesh& m = in.meshes[mi];
+    any = any || (!m.nodes && !m.bbs && !m.prim_idxs);
+  }
+  if (!any) return LGPU_OK;
+  ctx->built.resize(in.n_meshes);
+  ctx->patched.assign(in.meshes, in.meshes + in.n_meshes);
+  for (uint32_t mi = 0; mi < in.n_meshes; mi++) {
+    lgpu_mesh& m = ctx->patched[mi];
+    if (m.nodes || m.bbs || m.prim_idxs) continue;
+    std::string const what = "mesh " + std::to_string(mi) + ": ";
+    if (!m.V || !m.F || m.f_stride < 3 || m.n_faces == 0)
+      return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "incomplete mesh " + std::to_string(mi));
+    for (uint32_t f = 0; f < m.n_faces; f++)
+      for (int k = 0; k < 3; k++)
+        if (m.F[size_t(f) * m.f_stride + k] >= m.n_positions)
+          return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "face index out of range in mesh " + std::to_string(mi));
+    for (size_t i = 0; i < 3 * size_t(m.n_positions); i++)
+      if (!std::isfinite(m.V[i]))
+        return fail(ctx, LGPU_ERR_INVALID_ARGUMENT,
+                    what + "vertex " + std::to_string(i / 3) + " is not finite (no BVH can be built)");
+    RefBvh& B = ctx->built[mi];
+    cudaError_t e;
+    try {
+      e = build_bvh_device(m.V, m.n_positions, m.F, m.f_stride, m.n_faces, B, ctx->stream);
+    } catch (const std::bad_alloc&) {
+      return fail(ctx, LGPU_ERR_OUT_OF_MEMORY, what + "host memory for the BVH");
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "device BVH build");
+    m.nodes = B.nodes.data();
+    m.bbs = B.bbs.data();
+    m.prim_idxs = B.prim_idxs.data();
+    m.n_nodes = B.n_nodes;
+    m.n_bbs = uint32_t(B.bbs.size() / 48);
+    m.n_prim_idxs = uint32_t(B.prim_idxs.size());
+  }
+  out.meshes = ctx->patched.data();
+  return LGPU_OK;
+}
+
+int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene_in) {
+  lgpu_scene scene;
+  if (int r = build_missing_bvhs(ctx, scene_in, scene)) return r;
   HostLayout& L = ctx->layout;
   std::string err;
   bool const on_device = !(scene.flags & LGPU_SCENE_HOST_LAYOUT);

@@ -148,3 +148,29 @@ def test_device_layout_rejects_bad_indices(mixed_nls):
                 ctx.close()
         finally:
             arr[...] = saved
+
+
+def test_upload_builds_missing_bvh(mixed_nls):
+    """Meshes passed without their BVH (nodes, bbs, prim_idxs NULL) get the
+    tree bvh::build would make, built on the device at upload: traces and
+    renders are bit-identical to those of the scene with the reference's
+    trees."""
+    from lambda_b200.scene import FlatScene
+    from tests import raysets
+    sc = load_nls(mixed_nls)
+    rays = np.concatenate([raysets.camera_rays(sc, 48, seed=7),
+                           raysets.random_rays([-3, -3, 0.01], [3, 3, 3], 10000, seed=8)])
+    outs = []
+    for strip in (False, True):
+        flat = FlatScene(sc)
+        if strip:
+            for k in range(int(flat.scene.n_meshes)):
+                m = flat.meshes[k]
+                m.nodes, m.bbs, m.prim_idxs = None, None, None
+                m.n_nodes = m.n_bbs = m.n_prim_idxs = 0
+        ctx = Context()
+        ctx.upload(flat)
+        outs.append((ctx.trace(rays), ctx.render(8, 8, 0.8, seed=3)))
+        ctx.close()
+    assert np.array_equal(outs[0][0].view(np.uint8), outs[1][0].view(np.uint8))
+    assert np.array_equal(outs[0][1].view(np.uint32), outs[1][1].view(np.uint32))
