@@ -78,11 +78,32 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
       if (t[c] != 0.f) st.push(StackEntry{ref[c], t[c]});
     return true;
   }
-  int rank[8];
-  child_ranks(t, rank);
+  // Far to near by a sorting network on 32-bit keys: a hit's distance bits
+  // with their 3 low bits replaced by 7 - child (equal distances keep child
+  // order; a miss's key, 7 - child alone, is below every hit's).  19
+  // compare-exchanges of integer max/min cost fewer instructions than the
+  // pairwise ranks of push_children (measured: closest-hit traversal
+  // -1.4 %), and the hits are then pushed in sequence with their child
+  // references read again from the node (an L1 hit) instead of kept in
+  // registers.  The order can differ from the exact far-to-near order only
+  // between children whose entry distances lie within 8 ulps, which changes
+  // no closest distance (ties only; the reference-order traversal keeps
+  // push_children's exact order).  The stored distance is the key's, at
+  // most 7 ulps below the box's, so an entry is never culled early.
+  uint32_t key[8];
 #pragma unroll
-  for (int c = 0; c < 8; c++)
-    if (t[c] != 0.f) st.at(st.sp + rank[c]) = StackEntry{ref[c], t[c]};
+  for (int c = 0; c < 8; c++) key[c] = (t[c] != 0.f ? (__float_as_uint(t[c]) & ~7u) : 0u) | uint32_t(7 - c);
+  constexpr int kNet[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6}, {5, 7}, {1, 2}, {5, 6},
+                               {0, 4}, {3, 7}, {1, 5}, {2, 6}, {1, 4}, {3, 6}, {2, 4}, {3, 5}, {3, 4}};
+#pragma unroll
+  for (int k = 0; k < 19; k++) {
+    uint32_t const a = key[kNet[k][0]], b = key[kNet[k][1]];
+    key[kNet[k][0]] = max(a, b);
+    key[kNet[k][1]] = min(a, b);
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++)
+    if (j < hits) st.at(st.sp + j) = StackEntry{nd.child[7 - (key[j] & 7u)], __uint_as_float(key[j] & ~7u)};
   st.sp += hits;
   return true;
 }
