@@ -69,6 +69,8 @@ struct WaveState {
   uint8_t* s_vis;      // cap: 1 if the shadow ray reached its light
   uint32_t* s_job;     // cap (batched renders only)
   uint32_t* fb_queue;  // cap: `in` indices re-traced in the reference's object order
+  uint32_t* sort_key;  // cap + kMaxShadeBlock: each entry's place in its block's
+                       // material order and its group (the shading launches share one sort)
   uint32_t* ctl;       // kCtlWords counters
   uint32_t* h_ctl;     // pinned host copy of ctl
   float* sbuf;         // 3 per work item of a chunk: XYZ of every (sample, pixel)
