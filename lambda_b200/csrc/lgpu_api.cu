@@ -271,9 +271,7 @@ size_t wave_layout(uint8_t* base, uint32_t cap, uint32_t K, uint32_t npix, uint6
   ws.s_vis = c.take<uint8_t>(n);
   ws.s_job = batch ? c.take<uint32_t>(n) : nullptr;
   ws.fb_queue = c.take<uint32_t>(n);
-  // a shading block starts below the queue length and covers at most
-  // kMaxShadeBlock entries
-  ws.sort_key = c.take<uint32_t>(n + kMaxShadeBlock);
+  ws.shade_list = c.take<uint32_t>(n);
   ws.ctl = c.take<uint32_t>(kCtlWords);
   ws.film = c.take<float>(3 * size_t(npix));
   ws.film64 = fp64 ? c.take<double>(3 * size_t(npix)) : nullptr;

@@ -45,6 +45,8 @@ constexpr int kCtlNext = 7;      // next work item to start
 constexpr int kCtlNew = 8;       // plan of the next generate: new paths,
 constexpr int kCtlFirst = 9;     //   their first work item,
 constexpr int kCtlPos = 10;      //   their first queue position
+constexpr int kCtlListB = 11;    // queue entries that hit a Blinn material
+constexpr int kCtlListT = 12;    //   and a thin-film one (shading lists)
 constexpr int kCtlWords = 16;
 constexpr uint32_t kNoShadow = 0xFFFFFFFFu;
 
@@ -69,8 +71,8 @@ struct WaveState {
   uint8_t* s_vis;      // cap: 1 if the shadow ray reached its light
   uint32_t* s_job;     // cap (batched renders only)
   uint32_t* fb_queue;  // cap: `in` indices re-traced in the reference's object order
-  uint32_t* sort_key;  // cap + kMaxShadeBlock: each entry's place in its block's
-                       // material order and its group (the shading launches share one sort)
+  uint32_t* shade_list;  // cap: `in` positions of the Blinn hits (from the front) and
+                         // of the thin-film hits (from the back), for their shading launches
   uint32_t* ctl;       // kCtlWords counters
   uint32_t* h_ctl;     // pinned host copy of ctl
   float* sbuf;         // 3 per work item of a chunk: XYZ of every (sample, pixel)

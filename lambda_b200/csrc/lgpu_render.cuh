@@ -277,8 +277,9 @@ cudaError_t wave_chunk(const J& jobs, WaveState& w, uint64_t c0, uint32_t total,
     // one block per queue chunk, not persistent: a block's warps finish
     // their material-sorted groups at different times, and a persistent
     // block would hold the fast ones at the next chunk's sort barrier.
-    // Three launches, each with one material type's code (Blinn, thin
-    // film, the rest), so an SM's warps share their instructions.
+    // Three launches, each with one material type's code (the rest, Blinn,
+    // thin film), so an SM's warps share their instructions; the first
+    // lists the Blinn and thin-film hits for the other two.
     uint32_t const sg = (wi.cap + g.shade_block - 1) / g.shade_block;
     wf_shade<K, J, LGPU_MAT_LAMBERTIAN><<<sg, g.shade_block, 0, st>>>(jobs, wi, d_cnt);
     wf_shade<K, J, LGPU_MAT_BLINN><<<sg, g.shade_block, 0, st>>>(jobs, wi, d_cnt);

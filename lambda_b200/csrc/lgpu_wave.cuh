@@ -108,6 +108,8 @@ __global__ void wf_plan(WaveState w, uint32_t total) {
   w.ctl[kCtlFetch + 1] = 0;
   w.ctl[kCtlFallback] = 0;
   w.ctl[kCtlEnded] = 0;
+  w.ctl[kCtlListB] = 0;
+  w.ctl[kCtlListT] = 0;
 }
 
 // Starts the planned paths at the end of the queue: work item q is sample
@@ -335,11 +337,11 @@ __device__ __forceinline__ void shadow_done(const WaveState& w, uint32_t s, bool
 // them are waiting (12 of 32: 8, 10 and 16 were slower).
 constexpr int kRefill = 12;
 
-// Occupancy (measured best): 7 blocks of 128 per SM (72 registers) for
-// any-hit queries, 5 (96 registers, no spills with the row-wise box test and
-// the sorted push) for closest-hit queries.
+// Occupancy (measured best): 6 blocks of 128 per SM (80 registers) for
+// any-hit queries (7 and 8: +5 % and +3 % shadow time), 5 (96 registers) for
+// closest-hit queries; neither spills.
 template <bool ANY, int K, class J>
-__global__ void __launch_bounds__(128, ANY ? 7 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(128, ANY ? 6 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0, 0u};
@@ -534,6 +536,28 @@ __device__ __forceinline__ uint32_t material_order(const J& jobs, const WaveStat
   return r;
 }
 
+// After material_order: the block's Blinn entries are appended to the list
+// at the front of w.shade_list, its thin-film entries to the list growing
+// down from its end (both lists hold queue positions, together at most the
+// queue's length).  A group is a contiguous range of the block's threads,
+// so one atomic per list and block places it.
+__device__ __forceinline__ void list_material_groups(const WaveState& w, uint32_t i, uint32_t group) {
+  __shared__ uint32_t lbase[2];
+  uint32_t const gb = 1u + LGPU_MAT_BLINN, gt = 1u + LGPU_MAT_THINFILM;
+  uint32_t const below_b = uint32_t(__syncthreads_count(group < gb));
+  uint32_t const cnt_b = uint32_t(__syncthreads_count(group == gb));
+  uint32_t const below_t = uint32_t(__syncthreads_count(group < gt));
+  uint32_t const cnt_t = uint32_t(__syncthreads_count(group == gt));
+  if (threadIdx.x == 0) {
+    lbase[0] = cnt_b ? atomicAdd(w.ctl + kCtlListB, cnt_b) : 0u;
+    lbase[1] = cnt_t ? atomicAdd(w.ctl + kCtlListT, cnt_t) : 0u;
+  }
+  __syncthreads();
+  if (group == gb) w.shade_list[lbase[0] + threadIdx.x - below_b] = i;
+  if (group == gt) w.shade_list[w.cap - 1u - (lbase[1] + threadIdx.x - below_t)] = i;
+  __syncthreads();  // lbase is reused by the block's next chunk
+}
+
 // One vertex of Renderer::tracePath (src/renderer.cpp:64-146) for every
 // queued path: emitter hit (73-84), light importance sample with the MIS
 // power heuristic (87-113, its visibility left to the shadow kernel),
@@ -560,21 +584,23 @@ __global__ void __launch_bounds__(kMaxShadeBlock, 6) wf_shade(J jobs, WaveState 
   PathBuf const& in = w.in;
   PathBuf const& out = w.out;
   enum : int { kEnd = 0, kEmit = 1, kScatter = 2 };
-  for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+  // the Blinn and thin-film launches run over their lists (dense warps)
+  constexpr bool kList = MT == LGPU_MAT_BLINN || MT == LGPU_MAT_THINFILM;
+  uint32_t const n_loop = kList ? w.ctl[MT == LGPU_MAT_BLINN ? kCtlListB : kCtlListT] : n;
+  for (uint32_t base = blockIdx.x * blockDim.x; base < n_loop; base += gridDim.x * blockDim.x) {
     uint32_t group = 0;
-    // the three launches shade one material order: the first sorts the
-    // block's entries and records each thread's entry and group, the other
-    // two read them back instead of sorting again (the sort's chain of
-    // dependent loads, hit -> object -> material, is most of its cost;
-    // shading -5.5 %)
+    // the first launch sorts each block's entries by material and appends
+    // the Blinn and thin-film ones to the lists of the other two launches,
+    // which shade them with full warps instead of the quarter of each block
+    // that has their material (shading -24 % measured)
     uint32_t i;
-    if (MT == LGPU_MAT_BLINN || MT == LGPU_MAT_THINFILM) {
-      uint32_t const k = w.sort_key[base + threadIdx.x];
-      i = base + (k >> 8);
-      group = k & 0xFFu;
+    if (kList) {
+      uint32_t const j = base + threadIdx.x;
+      i = j < n_loop ? w.shade_list[MT == LGPU_MAT_BLINN ? j : cap - 1u - j] : UINT32_MAX;
+      group = 1u + MT;
     } else {
       i = material_order(jobs, w, base, n, &group);
-      if (MT == LGPU_MAT_LAMBERTIAN) w.sort_key[base + threadIdx.x] = ((i - base) << 8) | group;
+      if (MT == LGPU_MAT_LAMBERTIAN) list_material_groups(w, i, group);
     }
     bool const live = i < n && shade_group<MT>(group);
     uint32_t const jb = (J::kMulti && live) ? in.job[i] : 0u;
