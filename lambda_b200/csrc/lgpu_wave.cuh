@@ -574,11 +574,13 @@ __device__ __forceinline__ bool shade_group(uint32_t group) {
   return group != 1u + LGPU_MAT_BLINN && group != 1u + LGPU_MAT_THINFILM;
 }
 
-// Six blocks of 256 per SM (40 registers, with spills): the kernel waits on
-// memory, and more warps hide it better than registers save spill traffic
-// (4 blocks at 64 registers: +18 % shading time, 5: +2 %, 8: +5 %).
+// Six blocks of 256 per SM (40 registers, with spills) for the first
+// launch: the kernel waits on memory, and more warps hide it better than
+// registers save spill traffic (4 blocks at 64 registers: +18 % shading
+// time, 5: +2 %, 8: +5 %).  The list launches, whose warps are all busy,
+// run 5 (48 registers; 6 and 4: +0.6 % and +0 % shading time).
 template <int K, class J, int MT = -1>
-__global__ void __launch_bounds__(kMaxShadeBlock, 6) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(kMaxShadeBlock, (MT == LGPU_MAT_BLINN || MT == LGPU_MAT_THINFILM) ? 5 : 6) wf_shade(J jobs, WaveState w, DevCounters* cnt) {
   uint32_t const n = *w.n_in;
   uint32_t const cap = w.cap;
   PathBuf const& in = w.in;
