@@ -337,14 +337,16 @@ __device__ __forceinline__ void shadow_done(const WaveState& w, uint32_t s, bool
 // them are waiting (12 of 32: 8, 10 and 16 were slower).
 constexpr int kRefill = 12;
 
-// Occupancy (measured best): 6 blocks of 128 per SM (80 registers) for
-// any-hit queries (7 and 8: +5 % and +3 % shadow time), 5 (96 registers) for
-// closest-hit queries; neither spills.
+// Occupancy (measured best): 7 blocks of 128 per SM (72 registers) for
+// any-hit queries, 6 (80 registers) for closest-hit queries; the spills are a
+// few bytes.
 template <bool ANY, int K, class J>
-__global__ void __launch_bounds__(128, ANY ? 6 : 5) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
+__global__ void __launch_bounds__(128, ANY ? 7 : 6) wf_trace_persistent(J jobs, WaveState w, DevCounters* cnt) {
   extern __shared__ StackEntry smem_stack[];
   StackEntry lm[kLocalStack];
   SplitStack st{smem_stack + threadIdx.x, blockDim.x, lm, 0, 0u};
+  __shared__ float wsave[9 * 128];  // launched with 128 threads
+  st.ws = wsave + threadIdx.x;
   TravStats ts{0u, 0u, 0u, 0u};
   uint32_t rays = 0;
   uint32_t const n = ANY ? w.ctl[kCtlShadow] : *w.n_in;
