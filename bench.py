@@ -852,7 +852,11 @@ def run_device(args, w):
     e2e = {"value": job_throughput(paths_per_step, e2e_steps, world, e2e_s * 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(W * H * 3 * 4),
            "note": "lgpu_upload_scene (host layout + copies) + lgpu_render (kernel + image "
-                   "readback) per step"}
+                   "readback) per step; the meshes' BVHs (the reference's and the traversal "
+                   "tree) are built at scene load, as the reference builds its own (scene_build)"}
+    scene_build = tree_build_times(sc)
+    scene_build["e2e_with_traversal_tree_build"] = job_throughput(
+        paths_per_step, 1, world, e2e_s * 1e3 / e2e_steps + scene_build["traversal_tree_ms"])
 
     c = counters[-1]
     launches_per_step = int(c["launches"])
@@ -865,7 +869,7 @@ def run_device(args, w):
             "config": {"workload": workload_desc(w), "paths_per_step_per_gpu": paths_per_step,
                        "l2": "256 MB buffer written between timed steps",
                        "parallelism": "frame per GPU" if world > 1 else "single GPU"},
-            "e2e": e2e, "roofline": roofline, "clocks": clk,
+            "e2e": e2e, "scene_build": scene_build, "roofline": roofline, "clocks": clk,
             "gpu_launches": launches_per_step * args.steps,
             "mrays_per_s": world * c["rays"] * args.steps / (total_ms / 1e3) / 1e6}
     if rank == 0 and world == 1 and not args.no_baseline:
@@ -891,6 +895,22 @@ def run_device(args, w):
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def tree_build_times(sc, reps=3):
+    """Host time of the two BVH builds of the scene's largest mesh (median
+    of reps): the reference's tree (lgpu_build_bvh, bvh::build) and the
+    traversal tree (lgpu_build_traversal_bvh), both run by the loader."""
+    m = max(sc.meshes, key=lambda x: x.F.shape[0])
+    out = {"faces": int(m.F.shape[0]), "threads": os.cpu_count()}
+    for key, fn in (("reference_tree_ms", "lgpu_build_bvh"), ("traversal_tree_ms", "lgpu_build_traversal_bvh")):
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            m._tree(fn)
+            ts.append((time.perf_counter() - t0) * 1e3)
+        out[key] = float(statistics.median(ts))
+    return out
 
 
 def main():

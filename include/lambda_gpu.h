@@ -38,8 +38,12 @@ extern "C" {
    3: lgpu_stats gained local_stack; lgpu_trace_any,
    LGPU_FLAG_FP64_FILM and lgpu_scene.flags (LGPU_SCENE_HOST_LAYOUT) were
    added; lgpu_trace_closest runs the render's traversal kernels; uploads
-   lay the meshes out on the device */
-#define LGPU_ABI_VERSION 3
+   lay the meshes out on the device
+   4: a surface-area-heuristic traversal tree per mesh for the instance-BVH
+   traversal: lgpu_mesh gained its optional arrays (trav_*),
+   lgpu_build_traversal_bvh builds it, lgpu_upload_scene builds the missing
+   ones; LGPU_SCENE_REFERENCE_BVH keeps the reference's trees */
+#define LGPU_ABI_VERSION 4
 
 typedef struct lgpu_ctx lgpu_ctx;
 
@@ -175,6 +179,14 @@ typedef struct lgpu_mesh {
   const uint32_t* nodes;
   const float* bbs;
   const uint32_t* prim_idxs;
+  /* Optional: the mesh's traversal tree, in the same layout, as
+     lgpu_build_traversal_bvh builds it over this mesh's faces (a loader
+     builds it with the reference's tree, at scene load).  NULL (counts 0):
+     lgpu_upload_scene builds it, unless LGPU_SCENE_REFERENCE_BVH. */
+  uint32_t n_trav_nodes, n_trav_bbs, n_trav_prim_idxs, reserved2;
+  const uint32_t* trav_nodes;
+  const float* trav_bbs;
+  const uint32_t* trav_prim_idxs;
 } lgpu_mesh;
 
 /* lgpu_scene.flags: lay the meshes out on the host (the relayout pass of
@@ -183,6 +195,15 @@ typedef struct lgpu_mesh {
    nodes, leaf triangles and shading records itself; both give identical
    device data. */
 #define LGPU_SCENE_HOST_LAYOUT 0x1u
+/* lgpu_scene.flags: keep the reference's mesh BVHs for every traversal.  By
+   default lgpu_upload_scene also builds, for each mesh, an 8-wide BVH with
+   the surface-area heuristic on the host, which the instance-BVH traversal
+   (the renders' default) enters instead: the same closest hits in fewer node
+   and triangle tests (at exactly equal distances another face can be
+   reported).  The reference-order traversal (LGPU_FLAG_REFERENCE_ORDER)
+   always uses the reference's trees.  With this flag the meshes' trav_*
+   arrays are ignored and none is built. */
+#define LGPU_SCENE_REFERENCE_BVH 0x2u
 
 typedef struct lgpu_scene {
   lgpu_camera cam;
@@ -510,6 +531,18 @@ int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
                    uint32_t f_stride, uint32_t n_faces, uint32_t* nodes,
                    uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
                    uint32_t* prim_idxs, uint32_t* n_prim_idxs);
+
+/* The traversal tree of one mesh (no counterpart in the reference, whose
+   traversal uses bvh::build's tree): an 8-wide BVH built with the
+   surface-area heuristic on the host threads, leaves of at most 2 faces, in
+   the layout and with the array bounds of lgpu_build_bvh.  The instance-BVH
+   traversal of the renders enters it instead of the reference's tree: the
+   same closest hits in fewer node and triangle tests.  Vertex positions of
+   the faces must be finite (else LGPU_ERR_INVALID_ARGUMENT). */
+int lgpu_build_traversal_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
+                             uint32_t f_stride, uint32_t n_faces, uint32_t* nodes,
+                             uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
+                             uint32_t* prim_idxs, uint32_t* n_prim_idxs);
 
 /* lgpu_build_bvh on the context's GPU (bvh::build, cg.hpp:632-749, one
    tree level per step): the same arguments, host arrays in and out, and a

@@ -79,7 +79,10 @@ class Mesh(ctypes.Structure):
                 ("bounds", ctypes.c_float * 6),
                 ("n_nodes", ctypes.c_uint32), ("n_bbs", ctypes.c_uint32),
                 ("n_prim_idxs", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
-                ("nodes", c_uint32_p), ("bbs", c_float_p), ("prim_idxs", c_uint32_p)]
+                ("nodes", c_uint32_p), ("bbs", c_float_p), ("prim_idxs", c_uint32_p),
+                ("n_trav_nodes", ctypes.c_uint32), ("n_trav_bbs", ctypes.c_uint32),
+                ("n_trav_prim_idxs", ctypes.c_uint32), ("reserved2", ctypes.c_uint32),
+                ("trav_nodes", c_uint32_p), ("trav_bbs", c_float_p), ("trav_prim_idxs", c_uint32_p)]
 
 
 class Scene(ctypes.Structure):
@@ -145,6 +148,7 @@ FLAG_KERNEL_TIMING = 0x4
 FLAG_FP64_FILM = 0x8
 # lgpu_scene.flags
 SCENE_HOST_LAYOUT = 0x1
+SCENE_REFERENCE_BVH = 0x2  # keep the reference's mesh BVHs for every traversal
 KERNEL_CLOSEST, KERNEL_SHADOW, KERNEL_SHADE = 0, 1, 2
 
 
@@ -178,12 +182,14 @@ SIGNATURES = {
                                             _vp, _vp, _vp]),
     "lgpu_build_bvh": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
                                       _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
+    "lgpu_build_traversal_bvh": (ctypes.c_int, [_vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
+                                                _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
     "lgpu_build_bvh_device": (ctypes.c_int, [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, ctypes.c_uint32,
                                              _vp, c_uint32_p, _vp, c_uint32_p, _vp, c_uint32_p]),
 }
 
 # LGPU_ABI_VERSION of include/lambda_gpu.h
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 _lib = None
 

@@ -24,7 +24,7 @@ CU_SOURCES = ["lgpu_api.cu", "lgpu_kernels.cu", "lgpu_trace.cu", "lgpu_render_k4
               "lgpu_render_k16.cu", "lgpu_batch_k4.cu", "lgpu_batch_k8.cu", "lgpu_batch_k16.cu",
               "lgpu_adjoint_k4.cu", "lgpu_adjoint_k8.cu", "lgpu_adjoint_k16.cu",
               "lgpu_noalloc.cu", "lgpu_probe.cu", "lgpu_bvh_build.cu", "lgpu_layout_dev.cu"]
-CPP_SOURCES = ["lgpu_layout.cpp"]
+CPP_SOURCES = ["lgpu_layout.cpp", "lgpu_sah.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -81,6 +81,12 @@ struct lgpu_ctx {
   // table pointing at them (build_missing_bvhs)
   std::vector<RefBvh> built;
   std::vector<lgpu_mesh> patched;
+  // each mesh's traversal tree (build_traversal_trees): the caller's arrays
+  // or a tree built here, kept until the next upload
+  std::vector<TravTree> trav_views;
+  std::vector<RefBvh> trav;
+  std::vector<PrimBox> trav_boxes;
+  std::vector<float> trav_cents;
   // batch tables (lgpu_render_batch)
   DevArray<DevJob> jobs;
   DevArray<uint64_t> job_items;
@@ -580,15 +586,27 @@ bool timing_requested(const lgpu_render_params* p) {
 int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene, uint64_t& bytes) {
   const DeviceLayoutWork& W = ctx->dev_layout;
   cudaStream_t const st = ctx->stream;
-  auto pieces = [](const lgpu_mesh& m, size_t (&sz)[8]) {
+  // a job's tree: the mesh's own BVH, or its traversal tree
+  struct Tree {
+    uint32_t n_nodes, n_bbs, n_prims;
+    const uint32_t* nodes;
+    const float* bbs;
+    const uint32_t* prims;
+  };
+  auto tree_of = [&](const DeviceMeshJob& j) {
+    const lgpu_mesh& m = scene.meshes[j.mesh];
+    if (!j.tree) return Tree{m.n_nodes, m.n_bbs, m.n_prim_idxs, m.nodes, m.bbs, m.prim_idxs};
+    return Tree{j.tree->n_nodes, j.tree->n_bbs, j.tree->n_prims, j.tree->nodes, j.tree->bbs, j.tree->prims};
+  };
+  auto pieces = [](const lgpu_mesh& m, const Tree& T, size_t (&sz)[8]) {
     sz[0] = 12 * size_t(m.n_positions);
     sz[1] = 12 * size_t(m.n_normals);
     sz[2] = 12 * size_t(m.n_faces);
     sz[3] = 4 * size_t(m.f_stride) * m.n_faces;
-    sz[4] = 8 * size_t(m.n_nodes);
-    sz[5] = 192 * size_t(m.n_bbs);
-    sz[6] = 4 * size_t(m.n_prim_idxs);
-    sz[7] = 4 * size_t(m.n_nodes);
+    sz[4] = 8 * size_t(T.n_nodes);
+    sz[5] = 192 * size_t(T.n_bbs);
+    sz[6] = 4 * size_t(T.n_prims);
+    sz[7] = 4 * size_t(T.n_nodes);
     size_t t = 0;
     for (size_t x : sz) t += (x + 255) & ~size_t(255);
     return t;
@@ -596,7 +614,7 @@ int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene
   size_t most = 0;
   for (const DeviceMeshJob& j : W.jobs) {
     size_t sz[8];
-    most = std::max(most, pieces(scene.meshes[j.mesh], sz));
+    most = std::max(most, pieces(scene.meshes[j.mesh], tree_of(j), sz));
   }
   cudaError_t e = ensure(ctx->raw, most);
   if (e == cudaSuccess) e = ensure(ctx->layout_err, 1);
@@ -604,14 +622,18 @@ int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene
   if (e != cudaSuccess) return cuda_fail(ctx, e, "mesh layout buffers");
   for (const DeviceMeshJob& j : W.jobs) {
     const lgpu_mesh& m = scene.meshes[j.mesh];
+    Tree const T = tree_of(j);
     size_t sz[8];
-    pieces(m, sz);
-    const void* src[8] = {m.V, m.N, m.GN, m.F, m.nodes, m.bbs, m.prim_idxs, W.childref.data() + j.childref_off};
+    pieces(m, T, sz);
+    const void* src[8] = {m.V, m.N, m.GN, m.F, T.nodes, T.bbs, T.prims, W.childref.data() + j.childref_off};
     void* dst[8];
     size_t off = 0;
     for (int k = 0; k < 8 && e == cudaSuccess; k++) {
       dst[k] = ctx->raw.ptr + off;
       off += (sz[k] + 255) & ~size_t(255);
+      // a traversal tree's job follows its mesh's own job: the mesh's
+      // arrays (pieces 0-3, at the same offsets) are still in place
+      if (j.tree && k < 4) continue;
       if (sz[k]) e = cudaMemcpyAsync(dst[k], src[k], sz[k], cudaMemcpyHostToDevice, st);
       bytes += sz[k];
     }
@@ -619,10 +641,10 @@ int build_meshes_on_device(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene
                     static_cast<const float*>(dst[2]), static_cast<const uint32_t*>(dst[3]),
                     static_cast<const uint32_t*>(dst[4]), static_cast<const float*>(dst[5]),
                     static_cast<const uint32_t*>(dst[6]), static_cast<const uint32_t*>(dst[7]),
-                    m.n_positions, m.n_normals, m.n_faces, m.f_stride, m.n_nodes, m.n_prim_idxs};
+                    m.n_positions, m.n_normals, m.n_faces, m.f_stride, T.n_nodes, T.n_prims};
     if (e == cudaSuccess)
-      e = build_mesh_layout(r, j.mesh, sl.nodes.ptr, sl.tris.ptr + j.slot_base, sl.shade.ptr + j.face_base,
-                            ctx->layout_err.ptr, st);
+      e = build_mesh_layout(r, j.mesh, sl.nodes.ptr, sl.tris.ptr + j.slot_base,
+                            j.tree ? nullptr : sl.shade.ptr + j.face_base, ctx->layout_err.ptr, st);
     // the next mesh's copies reuse ctx->raw: stream order puts them after
     // these kernels; the host's pageable copies return once staged
   }
@@ -679,14 +701,59 @@ int build_missing_bvhs(lgpu_ctx* ctx, const lgpu_scene& in, lgpu_scene& out) {
   return LGPU_OK;
 }
 
+// Each mesh's traversal tree, unless the scene keeps the reference's trees:
+// the caller's (lgpu_mesh::trav_*), or one built here (build_sah_bvh, leaves
+// of at most 2 faces: 1, 3, 4 and 8 were slower).  A mesh whose faces index
+// outside its positions, or whose triangles are not finite, gets none here:
+// the layout reports a bad index, and the reference's tree serves a
+// non-finite mesh as the reference's own traversal would.
+int build_traversal_trees(lgpu_ctx* ctx, const lgpu_scene& sc) {
+  ctx->trav_views.assign(sc.n_meshes, TravTree{});
+  ctx->trav.resize(sc.n_meshes);
+  if ((sc.flags & LGPU_SCENE_REFERENCE_BVH) || !sc.meshes) return LGPU_OK;
+  for (uint32_t mi = 0; mi < sc.n_meshes; mi++) {
+    const lgpu_mesh& m = sc.meshes[mi];
+    bool const any = m.trav_nodes || m.trav_bbs || m.trav_prim_idxs;
+    if (any) {
+      if (!m.trav_nodes || !m.trav_bbs || !m.trav_prim_idxs || m.n_trav_nodes == 0)
+        return fail(ctx, LGPU_ERR_INVALID_ARGUMENT, "incomplete traversal tree of mesh " + std::to_string(mi));
+      ctx->trav_views[mi] = TravTree{m.n_trav_nodes, m.n_trav_bbs, m.n_trav_prim_idxs,
+                                     m.trav_nodes,   m.trav_bbs,   m.trav_prim_idxs};
+      continue;
+    }
+    RefBvh& T = ctx->trav[mi];
+    T.n_nodes = 0;
+    if (!m.V || !m.F || m.f_stride < 3 || m.n_faces == 0) continue;
+    bool ok = true;
+    for (size_t f = 0; f < m.n_faces && ok; f++)
+      for (int k = 0; k < 3; k++) ok = ok && m.F[f * m.f_stride + k] < m.n_positions;
+    if (!ok) continue;
+    try {
+      triangle_prims(m.V, m.F, m.f_stride, m.n_faces, ctx->trav_boxes, ctx->trav_cents);
+      for (const PrimBox& b : ctx->trav_boxes)
+        for (int k = 0; k < 3 && ok; k++) ok = std::isfinite(b.inf[k]) && std::isfinite(b.sup[k]);
+      for (size_t i = 0; i < ctx->trav_cents.size() && ok; i++) ok = std::isfinite(ctx->trav_cents[i]);
+      if (!ok) continue;
+      build_sah_bvh(m.n_faces, ctx->trav_boxes.data(), ctx->trav_cents.data(), T, 2);
+    } catch (const std::bad_alloc&) {
+      T = RefBvh{};  // no host memory: the reference's tree serves
+      continue;
+    }
+    ctx->trav_views[mi] = TravTree{T.n_nodes, uint32_t(T.bbs.size() / 48), uint32_t(T.prim_idxs.size()),
+                                   T.nodes.data(), T.bbs.data(), T.prim_idxs.data()};
+  }
+  return LGPU_OK;
+}
+
 int upload_slot(lgpu_ctx* ctx, SceneSlot& sl, const lgpu_scene& scene_in) {
   lgpu_scene scene;
   if (int r = build_missing_bvhs(ctx, scene_in, scene)) return r;
+  if (int r = build_traversal_trees(ctx, scene)) return r;
   HostLayout& L = ctx->layout;
   std::string err;
   bool const on_device = !(scene.flags & LGPU_SCENE_HOST_LAYOUT);
   DeviceLayoutWork& W = ctx->dev_layout;
-  int const rc = make_layout(scene, L, err, on_device ? &W : nullptr);
+  int const rc = make_layout(scene, L, err, on_device ? &W : nullptr, &ctx->trav_views);
   if (rc != LGPU_OK) return fail(ctx, rc, err);
   cudaStream_t const st = ctx->stream;
   uint64_t bytes = 0;
@@ -1300,6 +1367,37 @@ int lgpu_build_bvh_device(lgpu_ctx* ctx, const float* V, uint32_t n_positions, c
   if (nodes) std::memcpy(nodes, B.nodes.data(), B.nodes.size() * sizeof(uint32_t));
   if (bbs) std::memcpy(bbs, B.bbs.data(), B.bbs.size() * sizeof(float));
   if (prim_idxs) std::memcpy(prim_idxs, B.prim_idxs.data(), B.prim_idxs.size() * sizeof(uint32_t));
+  return LGPU_OK;
+}
+
+int lgpu_build_traversal_bvh(const float* V, uint32_t n_positions, const uint32_t* F, uint32_t f_stride,
+                             uint32_t n_faces, uint32_t* nodes, uint32_t* n_nodes, float* bbs, uint32_t* n_bbs,
+                             uint32_t* prim_idxs, uint32_t* n_prim_idxs) {
+  if (!V || !F || f_stride < 3 || n_faces == 0 || !n_nodes || !n_bbs || !n_prim_idxs)
+    return LGPU_ERR_INVALID_ARGUMENT;
+  for (uint32_t f = 0; f < n_faces; f++)
+    for (int k = 0; k < 3; k++)
+      if (F[size_t(f) * f_stride + k] >= n_positions) return LGPU_ERR_INVALID_ARGUMENT;
+  try {
+    std::vector<PrimBox> boxes;
+    std::vector<float> cents;
+    triangle_prims(V, F, f_stride, n_faces, boxes, cents);
+    for (const PrimBox& b : boxes)
+      for (int k = 0; k < 3; k++)
+        if (!std::isfinite(b.inf[k]) || !std::isfinite(b.sup[k])) return LGPU_ERR_INVALID_ARGUMENT;
+    for (float c : cents)
+      if (!std::isfinite(c)) return LGPU_ERR_INVALID_ARGUMENT;
+    RefBvh B;
+    build_sah_bvh(n_faces, boxes.data(), cents.data(), B, 2);
+    *n_nodes = B.n_nodes;
+    *n_bbs = uint32_t(B.bbs.size() / 48);
+    *n_prim_idxs = uint32_t(B.prim_idxs.size());
+    if (nodes) std::memcpy(nodes, B.nodes.data(), B.nodes.size() * sizeof(uint32_t));
+    if (bbs) std::memcpy(bbs, B.bbs.data(), B.bbs.size() * sizeof(float));
+    if (prim_idxs) std::memcpy(prim_idxs, B.prim_idxs.data(), B.prim_idxs.size() * sizeof(uint32_t));
+  } catch (const std::bad_alloc&) {
+    return LGPU_ERR_OUT_OF_MEMORY;
+  }
   return LGPU_OK;
 }
 

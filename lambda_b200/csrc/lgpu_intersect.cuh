@@ -179,7 +179,7 @@ __device__ __forceinline__ float prev_float(float z) {
 // _mm256_max_ps(a,b) = a>b?a:b and _mm256_min_ps(a,b) = a<b?a:b (the second
 // operand wins on NaN); a miss returns 0.
 __device__ __forceinline__ float child_box_t(const WideNode& nd, int c, const Ray& r,
-                                             bool nx, bool ny, bool nz, float t_max) {
+                                             bool nx, bool ny, bool nz, float t_max, float slack = 1.f) {
   float const bminx = nx ? nd.hix[c] : nd.lox[c];
   float const bmaxx = nx ? nd.lox[c] : nd.hix[c];
   float const bminy = ny ? nd.hiy[c] : nd.loy[c];
@@ -198,7 +198,7 @@ __device__ __forceinline__ float child_box_t(const WideNode& nd, int c, const Ra
   // return what the reference's compare-and-select does
   tmin = fmaxf(fmaxf(fmaxf(tmin, dminx), dminy), dminz);
   tmax = fminf(fminf(fminf(tmax, dmaxx), dmaxy), dmaxz);
-  return tmin <= tmax ? tmin : 0.f;
+  return tmin <= tmax * slack ? tmin : 0.f;
 }
 
 // All 8 child boxes of a wide node at once (the results of child_box_t):
@@ -207,7 +207,8 @@ __device__ __forceinline__ float child_box_t(const WideNode& nd, int c, const Ra
 // finite or ±FLT_MAX, b - p is finite) and a ±0 never decides a hit (tmin
 // starts at kBias > 0), so fmaxf/fminf return what the reference's
 // compare-and-select does.
-__device__ __forceinline__ void node_boxes_t(const WideNode& nd, const Ray& r, float t_max, float (&t)[8]) {
+__device__ __forceinline__ void node_boxes_t(const WideNode& nd, const Ray& r, float t_max, float (&t)[8],
+                                             float slack = 1.f) {
   bool const nx = r.inv.x < 0.f, ny = r.inv.y < 0.f, nz = r.inv.z < 0.f;
   const float4* const nrx = reinterpret_cast<const float4*>(nx ? nd.hix : nd.lox);
   const float4* const frx = reinterpret_cast<const float4*>(nx ? nd.lox : nd.hix);
@@ -230,7 +231,7 @@ __device__ __forceinline__ void node_boxes_t(const WideNode& nd, const Ray& r, f
       float const tmax =
           fminf(fminf(fminf(t_max, ml(sb(bfx[k], r.p.x), r.inv.x)), ml(sb(bfy[k], r.p.y), r.inv.y)),
                 ml(sb(bfz[k], r.p.z), r.inv.z));
-      t[4 * h + k] = tmin <= tmax ? tmin : 0.f;
+      t[4 * h + k] = tmin <= tmax * slack ? tmin : 0.f;
     }
     // keeps the second half's loads after the first half's tests (fewer
     // live registers)

@@ -365,7 +365,8 @@ int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::st
   return LGPU_OK;
 }
 
-int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev) {
+int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev,
+                const std::vector<TravTree>* trav) {
   if (dev) {
     dev->jobs.clear();
     dev->childref.clear();
@@ -469,11 +470,42 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLay
       dm.node_base = j.node_base;
       dm.slot_base = j.slot_base;
       dm.face_base = j.face_base;
+      dm.trav_root = dm.root;
       dev->mesh_nodes += j.n_int;
       dev->mesh_slots += m.n_prim_idxs;
       dev->mesh_faces += m.n_faces;
       dev->jobs.push_back(j);
       L.max_stack = std::max(L.max_stack, dm.max_stack);
+      const TravTree* T = trav && mi < trav->size() && (*trav)[mi].n_nodes ? &(*trav)[mi] : nullptr;
+      if (T) {
+        // the traversal tree: its own nodes and leaf slots, the mesh's faces
+        RefView const R2{T->n_nodes, T->n_bbs, T->n_prims, T->nodes, T->bbs, T->prims};
+        DeviceMeshJob t{};
+        t.mesh = mi;
+        t.node_base = dev->mesh_nodes;
+        t.slot_base = dev->mesh_slots;
+        t.face_base = j.face_base;
+        t.childref_off = dev->childref.size();
+        t.tree = T;
+        dev->childref.resize(t.childref_off + R2.n_nodes);
+        uint32_t root2 = 0, stack2 = 0;
+        if (!relayout_meta(R2, t.node_base, t.slot_base, dev->childref.data() + t.childref_off, t.n_int, root2,
+                           stack2, err)) {
+          err = "mesh " + std::to_string(mi) + " traversal tree: " + err;
+          return LGPU_ERR_INVALID_ARGUMENT;
+        }
+        // a tree deeper than the traversal stack is dropped: the mesh's own
+        // tree serves
+        if (stack2 <= uint32_t(kStackCap)) {
+          dm.trav_root = root2;
+          dev->mesh_nodes += t.n_int;
+          dev->mesh_slots += R2.n_prims;
+          dev->jobs.push_back(t);
+          L.max_stack = std::max(L.max_stack, stack2);
+        } else {
+          dev->childref.resize(t.childref_off);
+        }
+      }
       L.meshes.push_back(dm);
       continue;
     }
@@ -510,29 +542,32 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLay
       return LGPU_ERR_UNSUPPORTED;
     }
     L.max_stack = std::max(L.max_stack, dm.max_stack);
+    // the leaf triangles of a tree whose leaves list the faces `prims`
+    auto fill_tris = [&](const uint32_t* prims, size_t n_prims, TriSlot* tris) {
+      parallel_for(n_prims, [&](size_t s0, size_t s1) {
+        for (size_t s = s0; s < s1; s++) {
+          uint32_t const f = prims[s];
+          const uint32_t* t = m.F + size_t(f) * m.f_stride;
+          TriSlot& ts = tris[s];
+          const float* a = m.V + 3 * size_t(t[0]);
+          const float* b = m.V + 3 * size_t(t[1]);
+          const float* c = m.V + 3 * size_t(t[2]);
+          for (int i = 0; i < 3; i++) {
+            ts.v0[i] = a[i];
+            ts.v1[i] = b[i];
+            ts.v2[i] = c[i];
+          }
+          std::memcpy(&ts.v0[3], &f, 4);
+          ts.v1[3] = 0.f;
+          ts.v2[3] = 0.f;
+        }
+      });
+    };
     size_t const tri0 = L.tris.size(), shade0 = L.shade.size();
     L.tris.resize(tri0 + m.n_prim_idxs);
     L.shade.resize(shade0 + m.n_faces);
-    TriSlot* const tris = L.tris.data() + tri0;
     FaceShade* const shades = L.shade.data() + shade0;
-    parallel_for(m.n_prim_idxs, [&](size_t s0, size_t s1) {
-      for (size_t s = s0; s < s1; s++) {
-        uint32_t const f = m.prim_idxs[s];
-        const uint32_t* t = m.F + size_t(f) * m.f_stride;
-        TriSlot& ts = tris[s];
-        const float* a = m.V + 3 * size_t(t[0]);
-        const float* b = m.V + 3 * size_t(t[1]);
-        const float* c = m.V + 3 * size_t(t[2]);
-        for (int i = 0; i < 3; i++) {
-          ts.v0[i] = a[i];
-          ts.v1[i] = b[i];
-          ts.v2[i] = c[i];
-        }
-        std::memcpy(&ts.v0[3], &f, 4);
-        ts.v1[3] = 0.f;
-        ts.v2[3] = 0.f;
-      }
-    });
+    fill_tris(m.prim_idxs, m.n_prim_idxs, L.tris.data() + tri0);
     parallel_for(m.n_faces, [&](size_t f0, size_t f1) {
       for (size_t f = f0; f < f1; f++) {
         const uint32_t* t = m.F + f * m.f_stride;
@@ -545,6 +580,37 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLay
         }
       }
     });
+    dm.trav_root = dm.root;
+    const TravTree* T = trav && mi < trav->size() && (*trav)[mi].n_nodes ? &(*trav)[mi] : nullptr;
+    if (T) {
+      // the traversal tree: its own nodes and leaf slots, the mesh's faces
+      RefView const R2{T->n_nodes, T->n_bbs, T->n_prims, T->nodes, T->bbs, T->prims};
+      size_t const nodes0 = L.nodes.size(), slot2 = L.tris.size();
+      uint32_t root2 = 0, stack2 = 0;
+      std::atomic<bool> bad_trav{false};
+      parallel_for(R2.n_prims, [&](size_t s0, size_t s1) {
+        for (size_t q = s0; q < s1; q++)
+          if (R2.prims[q] >= m.n_faces) bad_trav = true;
+      });
+      if (bad_trav) {
+        err = "traversal-tree primitive index out of range in mesh " + std::to_string(mi);
+        return LGPU_ERR_INVALID_ARGUMENT;
+      }
+      if (!relayout(R2, 0, uint32_t(slot2), L.nodes, root2, stack2, err)) {
+        err = "mesh " + std::to_string(mi) + " traversal tree: " + err;
+        return LGPU_ERR_INVALID_ARGUMENT;
+      }
+      // a tree deeper than the traversal stack is dropped: the mesh's own
+      // tree serves
+      if (stack2 <= uint32_t(kStackCap)) {
+        L.tris.resize(slot2 + R2.n_prims);
+        fill_tris(R2.prims, R2.n_prims, L.tris.data() + slot2);
+        dm.trav_root = root2;
+        L.max_stack = std::max(L.max_stack, stack2);
+      } else {
+        L.nodes.resize(nodes0);
+      }
+    }
     L.meshes.push_back(dm);
   }
   // objects and their world boxes

@@ -20,6 +20,15 @@ struct RefBvh {
   uint32_t n_nodes = 0, n_interior = 0;
 };
 
+// A wide BVH in the reference's format, by reference (a mesh's traversal
+// tree: the caller's arrays or one built at upload).  n_nodes 0: none.
+struct TravTree {
+  uint32_t n_nodes = 0, n_bbs = 0, n_prims = 0;
+  const uint32_t* nodes = nullptr;
+  const float* bbs = nullptr;
+  const uint32_t* prims = nullptr;
+};
+
 struct PrimBox {
   float inf[3], sup[3];
 };
@@ -29,6 +38,13 @@ struct PrimBox {
 // reference's PRIM_PER_LEAF = 4 for meshes).
 void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out,
                    size_t max_leaf = 4);
+
+// The traversal tree of a mesh (lgpu_sah.cpp): an 8-wide BVH over the same
+// primitive boxes built with the surface-area heuristic, in the same
+// format; leaves hold at most max_leaf primitives.  Boxes and centroids must
+// be finite.
+void build_sah_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out,
+                   size_t max_leaf = 2);
 
 // Boxes and centroids of triangle faces as trimeshdata::aabboftri and
 // centroidoftri compute them (cg.hpp:776-790).
@@ -95,6 +111,9 @@ struct DeviceMeshJob {
   uint32_t node_base, n_int;      // its first WideNode and their number
   uint32_t slot_base, face_base;  // its first TriSlot and FaceShade
   size_t childref_off;            // its child references in DeviceLayoutWork::childref
+  // the mesh's traversal tree instead of its own BVH (no shading records:
+  // the job of the mesh's own BVH, just before this one, writes them)
+  const TravTree* tree = nullptr;
 };
 struct DeviceLayoutWork {
   std::vector<DeviceMeshJob> jobs;
@@ -110,7 +129,11 @@ struct DeviceLayoutWork {
 // follow the meshes' dev->mesh_nodes nodes), L.tris and L.shade stay
 // empty, and dev lists what build_mesh_layout has to build; the face and
 // primitive indices are checked there.
-int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev = nullptr);
+// trav, if given, holds per mesh its traversal tree (n_nodes 0: none), laid
+// out after the mesh's own tree; DevMesh::trav_root is its root,
+// or the mesh's own root without one.
+int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLayoutWork* dev = nullptr,
+                const std::vector<TravTree>* trav = nullptr);
 
 // The validated material table alone (for lgpu_update_materials).
 int make_materials(const lgpu_scene& sc, std::vector<DevMaterial>& mats, std::string& err);

@@ -102,7 +102,7 @@ cudaError_t build_mesh_layout(const MeshRaw& m, uint32_t mesh, WideNode* nodes, 
                               uint32_t* err, cudaStream_t st) {
   if (m.n_nodes) k_mesh_nodes<<<(m.n_nodes + 255) / 256, 256, 0, st>>>(m, nodes);
   if (m.n_prims) k_mesh_tris<<<(m.n_prims + 255) / 256, 256, 0, st>>>(m, mesh, tris, err);
-  if (m.n_faces) k_mesh_shade<<<(m.n_faces + 255) / 256, 256, 0, st>>>(m, mesh, shade, err);
+  if (m.n_faces && shade) k_mesh_shade<<<(m.n_faces + 255) / 256, 256, 0, st>>>(m, mesh, shade, err);
   return cudaGetLastError();
 }
 

@@ -26,7 +26,8 @@ struct MeshRaw {
 // childref holds global indices), its leaf triangles into tris (its first
 // slot) and its shading records into shade (its first face).  *err is
 // lowered to mesh * 4 + 1 (a face index out of range) or + 2 (a BVH
-// primitive index out of range).
+// primitive index out of range).  With shade NULL the shading records are
+// not written (a second tree of a mesh whose records exist).
 cudaError_t build_mesh_layout(const MeshRaw& m, uint32_t mesh, WideNode* nodes, TriSlot* tris, FaceShade* shade,
                               uint32_t* err, cudaStream_t st);
 

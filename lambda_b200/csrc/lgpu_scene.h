@@ -78,6 +78,10 @@ struct DevMesh {
   uint32_t slot_base;   // first TriSlot
   uint32_t face_base;   // first FaceShade
   uint32_t root;        // child reference of the root (node or leaf)
+  // the root of the traversal tree the instance-BVH traversal enters: a
+  // surface-area-heuristic tree in the same node and slot arrays, or `root`
+  // (the reference's tree, which the reference-order traversal enters)
+  uint32_t trav_root;
   float bounds[6];      // trimeshdata::bounds (inf, sup)
   uint32_t n_faces;
   uint32_t max_stack;   // traversal stack entries this mesh can need

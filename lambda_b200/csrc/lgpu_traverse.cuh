@@ -20,6 +20,17 @@
 
 namespace lgpu {
 
+// The instance-BVH traversal tests boxes with a relative slack: a child is
+// kept while its rounded entry distance is at most (1 + 2^-16) times its
+// rounded exit (the closest hit so far included), and a popped entry is
+// dropped only beyond (1 + 2^-16) times the closest hit.  A box's rounded
+// entry can lie a few ulps beyond a triangle it contains (its vertex on the
+// box's face), and without the slack such a triangle can be culled when a
+// neighbouring one was hit first (one ray of 1.14 million in the benchmark
+// scene traced with the surface-area-heuristic trees).  The slack only adds
+// node tests; the reference-order traversal keeps the exact test.
+constexpr float kTravSlack = 1.f + 1.f / 65536.f;
+
 constexpr int kSmemStack = 16;
 constexpr int kLocalStack = kStackCap + kTlasStackCap + 4 - kSmemStack;
 constexpr uint32_t kMarker = 0xFFFFFFFEu;
@@ -72,7 +83,7 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
   // ROWS: the row-wise test (the persistent kernels, which have the
   // registers for it); otherwise the per-child test (both give the same t)
   if (ROWS) {
-    node_boxes_t(nd, r, t_max, t);
+    node_boxes_t(nd, r, t_max, t, kTravSlack);
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       ref[c] = nd.child[c];
@@ -83,7 +94,7 @@ __device__ __forceinline__ bool push_children_split(const WideNode& nd, const Ra
 #pragma unroll
     for (int c = 0; c < 8; c++) {
       ref[c] = nd.child[c];
-      t[c] = (ref[c] != kEmptyChild) ? child_box_t(nd, c, r, nx, ny, nz, t_max) : 0.f;
+      t[c] = (ref[c] != kEmptyChild) ? child_box_t(nd, c, r, nx, ny, nz, t_max, kTravSlack) : 0.f;
     }
   }
   int hits = 0;
@@ -172,7 +183,7 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
       lowered = false;
       continue;
     }
-    if (e.t > h.z) continue;
+    if (e.t > h.z * kTravSlack) continue;
     if (!(e.ref & kLeafBit)) {
       ts.nodes++;
       if (!push_children_split<ANY>(S.nodes[e.ref], in_mesh ? l : w, h.z, st, !ANY)) {
@@ -265,7 +276,7 @@ __device__ __forceinline__ bool trace_tlas(const DevScene& S, const Ray& w, HitR
     lowered = low;
     in_mesh = true;
     st.push(StackEntry{kMarker, 0.f});
-    st.push(StackEntry{m.root, r0});
+    st.push(StackEntry{m.trav_root, r0});
   }
   return hit_any;
 }
@@ -325,7 +336,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
     t.w.inv = f3{st.ws[6 * 128], st.ws[7 * 128], st.ws[8 * 128]};
     return st.sp == 0;
   }
-  if (e.t > h.z) return st.sp == 0;
+  if (e.t > h.z * kTravSlack) return st.sp == 0;
   if (!(e.ref & kLeafBit)) {
     ts.nodes++;
     // children near to far, except in the shadow kernel: its answer does not
@@ -431,7 +442,7 @@ __device__ __forceinline__ bool trace_step(const DevScene& S, TraceState& t, Spl
   t.lowered = low;
   t.in_mesh = true;
   st.push(StackEntry{kMarker, 0.f});
-  st.push(StackEntry{m.root, r0});
+  st.push(StackEntry{m.trav_root, r0});
   return false;
 }
 

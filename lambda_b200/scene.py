@@ -351,21 +351,29 @@ class TriMeshData:
 
     def build_bvh(self):
         """trimeshdata::buildBVH (cg.hpp:792) through the library's
-        restatement of bvh::build."""
+        restatement of bvh::build, and the mesh's traversal tree
+        (lgpu_build_traversal_bvh: the tree the renders' instance-BVH
+        traversal enters), both at load as the reference builds its tree.
+        The traversal tree is skipped for meshes with non-finite vertices
+        (the upload then traverses the reference's tree)."""
+        self.nodes, self.bbs, self.prim_idxs = self._tree("lgpu_build_bvh")
+        try:
+            self.trav_nodes, self.trav_bbs, self.trav_prim_idxs = self._tree("lgpu_build_traversal_bvh")
+        except L.LgpuError:
+            self.trav_nodes = self.trav_bbs = self.trav_prim_idxs = None
+
+    def _tree(self, fn):
         nf = self.F.shape[0]
-        lib = L.lib()
         nodes = np.zeros(4 * nf + 4, np.uint32)
         bbs = np.zeros(96 * nf + 96, np.float32)
         prims = np.zeros(nf + 1, np.uint32)
         nn, nb, npi = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-        rc = lib.lgpu_build_bvh(self.V.ctypes.data, self.V.shape[0], self.F.ctypes.data, 6, nf,
-                                nodes.ctypes.data, ctypes.byref(nn), bbs.ctypes.data,
-                                ctypes.byref(nb), prims.ctypes.data, ctypes.byref(npi))
+        rc = getattr(L.lib(), fn)(self.V.ctypes.data, self.V.shape[0], self.F.ctypes.data, 6, nf,
+                                  nodes.ctypes.data, ctypes.byref(nn), bbs.ctypes.data,
+                                  ctypes.byref(nb), prims.ctypes.data, ctypes.byref(npi))
         if rc != 0:
-            raise L.LgpuError(rc, "lgpu_build_bvh failed")
-        self.nodes = nodes[:2 * nn.value].copy()
-        self.bbs = bbs[:48 * nb.value].copy()
-        self.prim_idxs = prims[:npi.value].copy()
+            raise L.LgpuError(rc, fn + " failed")
+        return nodes[:2 * nn.value].copy(), bbs[:48 * nb.value].copy(), prims[:npi.value].copy()
 
 
 def face_normals(V, F):
@@ -787,6 +795,11 @@ class FlatScene:
             d.n_nodes, d.n_bbs, d.n_prim_idxs = (m.nodes.size // 2, m.bbs.size // 48,
                                                  m.prim_idxs.size)
             d.nodes, d.bbs, d.prim_idxs = _up(m.nodes), _fp(m.bbs), _up(m.prim_idxs)
+            if getattr(m, "trav_nodes", None) is not None:
+                d.n_trav_nodes, d.n_trav_bbs, d.n_trav_prim_idxs = (m.trav_nodes.size // 2,
+                                                                    m.trav_bbs.size // 48, m.trav_prim_idxs.size)
+                d.trav_nodes, d.trav_bbs = _up(m.trav_nodes), _fp(m.trav_bbs)
+                d.trav_prim_idxs = _up(m.trav_prim_idxs)
         cmf = cie_tables(cfg)
         self.cmf = [np.ascontiguousarray(cmf[i]) for i in range(3)]
         s = L.Scene()
