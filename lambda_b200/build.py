@@ -76,8 +76,8 @@ def build(force=False, verbose=False, extra_flags=()):
         objs.append(obj)
     for src in CPP_SOURCES:
         obj = os.path.join(BUILD_DIR, src + ".o")
-        cmds.append([nvcc()] + common + ["-Xcompiler", "-pthread", "-x", "c++", "-c", os.path.join(CSRC, src),
-                                         "-o", obj])
+        cmds.append([nvcc()] + common + extra_flags + ["-Xcompiler", "-pthread", "-x", "c++", "-c",
+                                                       os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     procs = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.STDOUT) for c in cmds]
     logs = []

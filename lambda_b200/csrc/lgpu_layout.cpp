@@ -669,8 +669,12 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLay
   }
   if (sc.n_objects > 0) {
     RefBvh tl;
-    // one object per leaf: objects are culled by the 8-wide box test
-    build_ref_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
+    // one object per leaf: objects are culled by the 8-wide box test.  Only
+    // the instance-BVH traversal enters it (the reference order loops over
+    // the objects), so it is built with the surface-area heuristic: 9.4
+    // node tests per ray instead of 12.0 with the reference's split rule on
+    // the benchmark scene (frame +10.5 %, measured)
+    build_sah_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
     L.tlas_objects = tl.prim_idxs;
     RefView const R{tl.n_nodes, uint32_t(tl.bbs.size() / 48), uint32_t(tl.prim_idxs.size()),
                     tl.nodes.data(), tl.bbs.data(), tl.prim_idxs.data()};
