@@ -668,24 +668,35 @@ int make_layout(const lgpu_scene& sc, HostLayout& L, std::string& err, DeviceLay
     L.tlas_bounds[3 + k] = -1e30f;
   }
   if (sc.n_objects > 0) {
-    RefBvh tl;
     // one object per leaf: objects are culled by the 8-wide box test.  Only
     // the instance-BVH traversal enters it (the reference order loops over
     // the objects), so it is built with the surface-area heuristic: 9.4
     // node tests per ray instead of 12.0 with the reference's split rule on
-    // the benchmark scene (frame +10.5 %, measured)
-    build_sah_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
-    L.tlas_objects = tl.prim_idxs;
-    RefView const R{tl.n_nodes, uint32_t(tl.bbs.size() / 48), uint32_t(tl.prim_idxs.size()),
-                    tl.nodes.data(), tl.bbs.data(), tl.prim_idxs.data()};
-    // after the meshes' nodes, wherever those are built
-    if (!relayout(R, dev ? dev->mesh_nodes : 0, 0, L.nodes, L.tlas_root, L.tlas_max_stack, err)) {
-      err = "instance BVH: " + err;
-      return LGPU_ERR_INVALID_ARGUMENT;
-    }
-    if (L.tlas_max_stack > uint32_t(kTlasStackCap)) {
-      err = "instance BVH can need " + std::to_string(L.tlas_max_stack) + " stack entries";
-      return LGPU_ERR_UNSUPPORTED;
+    // the benchmark scene (frame +10.5 %, measured).  A tree whose stack
+    // bound exceeds the traversal's instance stack (thousands of objects
+    // can) is replaced by the reference's split rule, whose 8-way slabs
+    // give shallower trees.
+    size_t const nodes0 = L.nodes.size();
+    for (int attempt = 0; attempt < 2; attempt++) {
+      RefBvh tl;
+      if (attempt == 0)
+        build_sah_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
+      else
+        build_ref_bvh(sc.n_objects, boxes.data(), cents.data(), tl, 1);
+      L.tlas_objects = tl.prim_idxs;
+      RefView const R{tl.n_nodes, uint32_t(tl.bbs.size() / 48), uint32_t(tl.prim_idxs.size()),
+                      tl.nodes.data(), tl.bbs.data(), tl.prim_idxs.data()};
+      L.nodes.resize(nodes0);
+      // after the meshes' nodes, wherever those are built
+      if (!relayout(R, dev ? dev->mesh_nodes : 0, 0, L.nodes, L.tlas_root, L.tlas_max_stack, err)) {
+        err = "instance BVH: " + err;
+        return LGPU_ERR_INVALID_ARGUMENT;
+      }
+      if (L.tlas_max_stack <= uint32_t(kTlasStackCap)) break;
+      if (attempt == 1) {
+        err = "instance BVH can need " + std::to_string(L.tlas_max_stack) + " stack entries";
+        return LGPU_ERR_UNSUPPORTED;
+      }
     }
     PrimBox all;
     box_init(all);

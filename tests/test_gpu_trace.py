@@ -82,6 +82,29 @@ def test_closest_hit_instance_bvh(which, request):
     assert diff.sum() <= max(1, len(rays) // 10000)
 
 
+def test_many_objects_instance_bvh(scene_dir):
+    """4,160 objects (the inverse-rendering scene: one quad per albedo and
+    per thickness tile).  Its surface-area-heuristic instance BVH needs more
+    entries than the traversal's instance stack holds, so the upload builds
+    that level with the reference's split rule instead; distances stay
+    bit-identical to intersect::scene."""
+    from lambda_b200 import synth
+    alb = np.full((64, synth.ALBEDO_BINS), 0.5)
+    th = np.full((64, 64), 400.0)
+    nls = synth.diff_scene(str(scene_dir / "diff64"), alb, th, width=64)
+    sc = load_nls(nls)
+    ref = refharness.RefScene(nls)
+    rays = _rays(sc, ref)
+    r = ref.intersect(rays)
+    assert (r["obj"] != MISS).sum() > len(rays) // 4
+    ctx = Context()
+    ctx.upload(sc)
+    g = ctx.trace(rays)
+    assert np.array_equal(_bits(g["t"]), _bits(r["t"]))
+    assert ctx.stats()["device_checks"] == 0
+    ctx.close()
+
+
 def test_trace_empty_and_miss(mixed_nls):
     sc = load_nls(mixed_nls)
     ctx = Context()
