@@ -286,7 +286,6 @@ class Builder {
     uint32_t const n = r.size();
     Prim* const first = prims.data() + r.b;
     double best = 1e300;
-    int best_k = 0;
     uint32_t best_at = n / 2;
     Prim sorted[kSmall], keep[kSmall];
     double right_area[kSmall];
@@ -312,7 +311,6 @@ class Builder {
         double const cost = acc.area() * i + right_area[i] * (n - i);
         if (cost < best) {
           best = cost;
-          best_k = k;
           best_at = i;
           better = true;
         }
