@@ -4,25 +4,26 @@
 //
 // The reference's builder (bvh::build, cg.hpp:632-749) splits every node
 // into 8 equal-width centroid bins along its longest axis, so a node's
-// children are slabs along one axis; a ray crosses many of them.  Here each
-// node gets up to 8 children by repeated binary splits: the child with the
-// largest surface area is split where the surface-area cost (the
-// area-weighted primitive counts of the two sides) is lowest, until there
-// are 8 children or none can split: over 32 centroid bins on the axis of the
-// largest centroid extent (binning all three axes took 2.1x the build time
-// for a tree that traced no faster; 32 bins traced 0.45 % faster than 16,
-// measured), or, for at most 24
-// primitives, over every split of their centroid order on each axis.  Leaves hold at most
-// max_leaf primitives.  The closest hit along a ray does not depend on the
-// tree (the triangle test is the same exact test); only which of two faces at
-// exactly equal distance is reported can.  The reference's own tree is kept
-// for the reference-order traversal.
+// children are slabs along one axis; a ray crosses many of them.  Here a
+// binary tree is built top-down, each range split where the surface-area
+// cost (the area-weighted primitive counts of the two sides) is lowest: over
+// 32 centroid bins on the axis of the largest centroid extent (binning all
+// three axes took 2.1x the build time for a tree that traced no faster; 32
+// bins traced 0.45 % faster than 16, measured), or, for at most 24
+// primitives, over every split of their centroid order on each axis.  The
+// binary tree is then collapsed into wide nodes of up to 8 children and
+// leaves of up to max_leaf primitives by the cost-optimal dynamic program
+// of Ylitie, Karras and Laine (HPG 2017): frame +1.2 % against opening the
+// child of largest area until there are 8, measured.  The closest hit along
+// a ray does not depend on the tree (the triangle test is the same exact
+// test); only which of two faces at exactly equal distance is reported can.
+// The reference's own tree is kept for the reference-order traversal.
 //
 // A binned split visits its primitives twice: once to bin them, once to
 // partition them (the children's centroid bounds on the way); the
-// children's boxes come from the bins.  Subtrees of more than
-// kSpawn primitives are queued for the worker threads, each of which keeps
-// the nodes it builds.
+// children's boxes come from the bins.  Subtrees of more than kSpawn
+// primitives are queued for the worker threads, each of which keeps the
+// nodes it builds and costs them on the way up.
 #include <algorithm>
 #include <cmath>
 #include <condition_variable>
@@ -70,16 +71,84 @@ struct Range {
   uint32_t size() const { return e - b; }
 };
 
-// A node of the build tree: a leaf (primitives prims[b, e)) or up to 8
-// children, referenced as (worker << 24) | index in that worker's nodes.
+// A node of the binary build tree over primitives prims[b, e): one
+// primitive, or two children referenced as (worker << 24) | index in that
+// worker's nodes.  C[i] is the least cost of the subtree as at most i + 1
+// roots of wide nodes or leaves (the dynamic program of Ylitie, Karras and
+// Laine, "Efficient Incoherent Ray Traversal on GPUs Through Compressed
+// Wide BVHs", HPG 2017), with the choice that reaches it: D[i] = kOneLeaf
+// or kOneNode (one root: this node as a leaf, or as a wide node whose
+// children split 8 roots K[0] / 8 - K[0] between its two children),
+// kSplit (K[i] roots from the first child, the rest from the second) or
+// kFewer (as with i roots).
+enum : uint8_t { kOneLeaf = 0, kOneNode = 1, kSplit = 2, kFewer = 3 };
 struct BNode {
   Box box;
   uint32_t b = 0, e = 0;
-  uint32_t kid[8];
-  uint8_t nk = 0;
-  bool leaf = false;
+  uint32_t kid[2] = {0, 0};
+  bool leaf = false;    // a single primitive
+  bool costed = false;  // C, D and K are set
+  float C[8];
+  uint8_t D[8], K[8];
 };
 constexpr uint32_t kLocalBits = 24;
+// the costs of the dynamic program: a wide node's box tests and a leaf's
+// triangle tests per unit of surface area (the best of the costs measured:
+// 0.3 against 0.5 per face, leaves of at most 2 faces against 3)
+constexpr float kCostNode = 1.f, kCostFace = 0.3f, kCostInf = 1e30f;
+
+// C, D and K of nd from its children's
+void dp_cost(BNode& nd, const BNode* kid0, const BNode* kid1, size_t max_leaf) {
+  uint32_t const n = nd.e - nd.b;
+  float const area = float(nd.box.area());
+  float const leaf = n <= max_leaf ? area * kCostFace * float(n) : kCostInf;
+  if (nd.leaf) {
+    for (int i = 0; i < 8; i++) {
+      nd.C[i] = leaf;
+      nd.D[i] = i == 0 ? kOneLeaf : kFewer;
+      nd.K[i] = 0;
+    }
+    nd.costed = true;
+    return;
+  }
+  // dist[j - 1]: the least cost of j roots split between the children
+  float dist[8];
+  uint8_t dk[8];
+  for (int j = 0; j < 8; j++) {
+    dist[j] = kCostInf;
+    dk[j] = 0;
+  }
+  for (int j = 2; j <= 8; j++)
+    for (int k = 1; k < j; k++) {
+      float const v = kid0->C[k - 1] + kid1->C[j - k - 1];
+      if (v < dist[j - 1]) {
+        dist[j - 1] = v;
+        dk[j - 1] = uint8_t(k);
+      }
+    }
+  float const node = area * kCostNode + dist[7];
+  if (leaf <= node) {
+    nd.C[0] = leaf;
+    nd.D[0] = kOneLeaf;
+    nd.K[0] = 0;
+  } else {
+    nd.C[0] = node;
+    nd.D[0] = kOneNode;
+    nd.K[0] = dk[7];
+  }
+  for (int i = 2; i <= 8; i++) {
+    if (dist[i - 1] < nd.C[i - 2]) {
+      nd.C[i - 1] = dist[i - 1];
+      nd.D[i - 1] = kSplit;
+      nd.K[i - 1] = dk[i - 1];
+    } else {
+      nd.C[i - 1] = nd.C[i - 2];
+      nd.D[i - 1] = kFewer;
+      nd.K[i - 1] = 0;
+    }
+  }
+  nd.costed = true;
+}
 
 // a primitive's box, centroid and index
 struct Prim {
@@ -331,35 +400,11 @@ class Builder {
     }
   }
 
-  // The children of a node over r: up to 8 ranges by repeated binary
-  // splits of the child with the largest surface area.
-  int collapse(const Range& r, Range (&kids)[8]) {
-    int nk = 1;
-    kids[0] = r;
-    while (nk < 8) {
-      int pick = -1;
-      double area = -1.0;
-      for (int c = 0; c < nk; c++) {
-        if (kids[c].size() <= max_leaf_) continue;
-        double const a = kids[c].box.area();
-        if (a > area) {
-          area = a;
-          pick = c;
-        }
-      }
-      if (pick < 0) break;
-      Range a, b;
-      split(kids[pick], a, b, threads_ > 1 && kids[pick].size() > kParallelBins);
-      kids[pick] = a;
-      kids[nk++] = b;
-    }
-    return nk;
-  }
-
   static constexpr uint32_t kParallelBins = 1u << 16;
   static constexpr uint32_t kSmall = 24;
 
   size_t max_leaf() const { return max_leaf_; }
+  unsigned threads() const { return threads_; }
 
  private:
   const PrimBox* boxes_;
@@ -384,6 +429,7 @@ class NodeStore {
     return nd;
   }
   const BNode& operator[](uint32_t i) const { return chunks_[i >> kChunkBits][i & ((1u << kChunkBits) - 1)]; }
+  BNode& at(uint32_t i) { return chunks_[i >> kChunkBits][i & ((1u << kChunkBits) - 1)]; }
 
  private:
   std::vector<std::unique_ptr<BNode[]>> chunks_;
@@ -437,30 +483,48 @@ class Pool {
     }
   }
 
-  // the subtree over r in worker w's nodes
+  // the binary subtree over r in worker w's nodes, costed unless a child
+  // went to the queue (cost_pending then costs it)
   uint32_t build(const Range& r, unsigned w) {
     NodeStore& mine = nodes_[w];
     uint32_t const ref = (uint32_t(w) << kLocalBits) | mine.size();
     BNode* nd = mine.add();
     *nd = BNode{};
     nd->box = r.box;
-    if (r.size() <= B_.max_leaf()) {
+    nd->b = r.b;
+    nd->e = r.e;
+    if (r.size() == 1) {
       nd->leaf = true;
-      nd->b = r.b;
-      nd->e = r.e;
+      dp_cost(*nd, nullptr, nullptr, B_.max_leaf());
       return ref;
     }
-    Range kids[8];
-    int const nk = B_.collapse(r, kids);
-    nd->nk = uint8_t(nk);
-    for (int c = 0; c < nk; c++) {
-      if (kids[c].size() > kSpawn)
+    Range kids[2];
+    B_.split(r, kids[0], kids[1], B_.threads() > 1 && r.size() > Builder::kParallelBins);
+    bool queued = false;
+    for (int c = 0; c < 2; c++) {
+      if (kids[c].size() > kSpawn) {
         push(Task{kids[c], nd, &nd->kid[c]});
-      else
+        queued = true;
+      } else {
         nd->kid[c] = build(kids[c], w);
+      }
     }
+    if (!queued) dp_cost(*nd, &node(nd->kid[0]), &node(nd->kid[1]), B_.max_leaf());
     return ref;
   }
+
+ public:
+  // Costs the nodes whose children were built by other workers (after run).
+  void cost_pending(uint32_t ref) {
+    BNode& nd = node_mut(ref);
+    if (nd.costed) return;
+    cost_pending(nd.kid[0]);
+    cost_pending(nd.kid[1]);
+    dp_cost(nd, &node(nd.kid[0]), &node(nd.kid[1]), B_.max_leaf());
+  }
+
+ private:
+  BNode& node_mut(uint32_t ref) { return nodes_[ref >> kLocalBits].at(ref & ((1u << kLocalBits) - 1)); }
 
   Builder& B_;
   std::vector<NodeStore> nodes_;
@@ -485,27 +549,51 @@ void build_sah_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
   B.init_prims(n, root);
   Pool P(B, workers);
   uint32_t const root_ref = P.run(root);
+  P.cost_pending(root_ref);
+  // the wide roots a binary subtree becomes with i of them (its decisions)
+  std::vector<uint32_t> roots;
+  auto roots_of = [&](auto& self, uint32_t ref, int i) -> void {
+    const BNode& nd = P.node(ref);
+    uint8_t const d = nd.D[i - 1];
+    if (d == kFewer) {
+      self(self, ref, i - 1);
+    } else if (d == kSplit) {
+      self(self, nd.kid[0], nd.K[i - 1]);
+      self(self, nd.kid[1], i - nd.K[i - 1]);
+    } else {
+      roots.push_back(ref);
+    }
+  };
   // breadth-first numbering in the reference's layout: an interior node's
   // children are consecutive nodes, a leaf's primitives consecutive entries
   // of prim_idxs, and a record of child boxes holds its unused slots as
   // empty boxes (cg.hpp:700-727).  The numbering on this thread, the
   // records on all.
+  // A wide node is a binary node that is one root: a leaf of its
+  // primitives (kOneLeaf) or a wide node whose children are the roots its
+  // two children become with K[0] and 8 - K[0] of them (kOneNode).
   std::vector<uint32_t> order;
-  std::vector<uint32_t> at;  // per node in order: its first child, or its first primitive
+  std::vector<uint32_t> at;   // per node in order: its first child, or its first primitive
   std::vector<uint32_t> rec;  // per node in order: its record of child boxes
+  std::vector<uint8_t> nkid;  // per node in order: its children
   order.push_back(root_ref);
   uint32_t n_rec = 0, n_prim = 0;
   for (size_t h = 0; h < order.size(); h++) {
     const BNode& nd = P.node(order[h]);
-    if (nd.leaf) {
+    if (nd.D[0] == kOneLeaf) {
       at.push_back(n_prim);
       rec.push_back(0xFFFFFFFFu);
+      nkid.push_back(0);
       n_prim += nd.e - nd.b;
       continue;
     }
+    roots.clear();
+    roots_of(roots_of, nd.kid[0], nd.K[0]);
+    roots_of(roots_of, nd.kid[1], 8 - nd.K[0]);
     at.push_back(uint32_t(order.size()));
     rec.push_back(n_rec++);
-    for (int c = 0; c < nd.nk; c++) order.push_back(nd.kid[c]);
+    nkid.push_back(uint8_t(roots.size()));
+    order.insert(order.end(), roots.begin(), roots.end());
   }
   size_t const nn = order.size();
   out.nodes.resize(2 * nn);
@@ -514,7 +602,7 @@ void build_sah_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
   auto fill = [&](size_t q0, size_t q1) {
     for (size_t q = q0; q < q1; q++) {
       const BNode& nd = P.node(order[q]);
-      if (nd.leaf) {
+      if (nkid[q] == 0) {
         out.nodes[2 * q] = 0xFFFFFFFFu;
         out.nodes[2 * q + 1] = (at[q] << 4) | ((nd.e - nd.b - 1) << 1) | 1u;
         for (uint32_t i = nd.b; i < nd.e; i++) out.prim_idxs[at[q] + (i - nd.b)] = B.prims[i].id;
@@ -522,14 +610,14 @@ void build_sah_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
       }
       float* bb = out.bbs.data() + 48 * size_t(rec[q]);
       for (int c = 0; c < 8; c++) {
-        const Box* kb = c < nd.nk ? &P.node(nd.kid[c]).box : nullptr;
+        const Box* kb = c < nkid[q] ? &P.node(order[at[q] + c]).box : nullptr;
         for (int k = 0; k < 3; k++) {
           bb[k * 8 + c] = kb ? kb->lo[k] : 1e30f;
           bb[24 + k * 8 + c] = kb ? kb->hi[k] : -1e30f;
         }
       }
       out.nodes[2 * q] = rec[q];
-      out.nodes[2 * q + 1] = (at[q] << 4) | (uint32_t(nd.nk - 1) << 1);
+      out.nodes[2 * q + 1] = (at[q] << 4) | (uint32_t(nkid[q] - 1) << 1);
     }
   };
   if (workers > 1) {
