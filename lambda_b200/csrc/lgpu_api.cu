@@ -735,8 +735,8 @@ int build_traversal_trees(lgpu_ctx* ctx, const lgpu_scene& sc) {
       for (size_t i = 0; i < ctx->trav_cents.size() && ok; i++) ok = std::isfinite(ctx->trav_cents[i]);
       if (!ok) continue;
       build_sah_bvh(m.n_faces, ctx->trav_boxes.data(), ctx->trav_cents.data(), T, 2);
-    } catch (const std::bad_alloc&) {
-      T = RefBvh{};  // no host memory: the reference's tree serves
+    } catch (const std::exception&) {
+      T = RefBvh{};  // no host memory or threads: the reference's tree serves
       continue;
     }
     ctx->trav_views[mi] = TravTree{T.n_nodes, uint32_t(T.bbs.size() / 48), uint32_t(T.prim_idxs.size()),
@@ -1397,6 +1397,8 @@ int lgpu_build_traversal_bvh(const float* V, uint32_t n_positions, const uint32_
     if (prim_idxs) std::memcpy(prim_idxs, B.prim_idxs.data(), B.prim_idxs.size() * sizeof(uint32_t));
   } catch (const std::bad_alloc&) {
     return LGPU_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception&) {
+    return LGPU_ERR_OUT_OF_MEMORY;  // no threads for the build
   }
   return LGPU_OK;
 }

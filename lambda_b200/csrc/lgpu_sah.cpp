@@ -25,6 +25,8 @@
 // primitives are queued for the worker threads, each of which keeps the
 // nodes it builds and costs them on the way up.
 #include <algorithm>
+#include <atomic>
+#include <exception>
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
@@ -440,14 +442,21 @@ class Pool {
  public:
   Pool(Builder& B, unsigned workers) : B_(B), nodes_(workers) {}
 
-  // The tree over r; returns its root's reference.
+  // The tree over r; returns its root's reference.  A worker that fails
+  // (no memory, no thread) stops taking subtrees; the failure is rethrown
+  // here once all workers have returned.
   uint32_t run(const Range& r) {
     uint32_t root = 0;
     push(Task{r, nullptr, &root});
     std::vector<std::thread> ts;
-    for (unsigned w = 1; w < nodes_.size(); w++) ts.emplace_back([this, w] { work(w); });
+    try {
+      for (unsigned w = 1; w < nodes_.size(); w++) ts.emplace_back([this, w] { work(w); });
+    } catch (...) {
+      // fewer workers: the ones started and this thread finish the queue
+    }
     work(0);
     for (auto& t : ts) t.join();
+    if (failed_) std::rethrow_exception(failure_);
     return root;
   }
 
@@ -477,7 +486,15 @@ class Pool {
         t = queue_.front();
         queue_.pop_front();
       }
-      *t.slot = build(t.r, w);
+      if (!failed_) {
+        try {
+          *t.slot = build(t.r, w);
+        } catch (...) {
+          std::lock_guard<std::mutex> g(mu_);
+          if (!failed_) failure_ = std::current_exception();
+          failed_ = true;
+        }
+      }
       std::lock_guard<std::mutex> g(mu_);
       if (--pending_ == 0) cv_.notify_all();
     }
@@ -532,6 +549,8 @@ class Pool {
   std::condition_variable cv_;
   std::deque<Task> queue_;
   size_t pending_ = 0;
+  std::atomic<bool> failed_{false};
+  std::exception_ptr failure_;
 };
 
 }  // namespace
