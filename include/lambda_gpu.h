@@ -534,8 +534,9 @@ int lgpu_build_bvh(const float* V, uint32_t n_positions, const uint32_t* F,
 
 /* The traversal tree of one mesh (no counterpart in the reference, whose
    traversal uses bvh::build's tree): an 8-wide BVH built with the
-   surface-area heuristic on the host threads, leaves of at most 2 faces, in
-   the layout and with the array bounds of lgpu_build_bvh.  The instance-BVH
+   surface-area heuristic on the host threads (a binary tree collapsed to
+   8-wide nodes and leaves of at most 2 faces by a cost-optimal dynamic
+   program), in the layout and with the array bounds of lgpu_build_bvh.  The instance-BVH
    traversal of the renders enters it instead of the reference's tree: the
    same closest hits in fewer node and triangle tests.  Vertex positions of
    the faces must be finite (else LGPU_ERR_INVALID_ARGUMENT). */

@@ -40,8 +40,9 @@ void build_ref_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, Ref
                    size_t max_leaf = 4);
 
 // The traversal tree of a mesh (lgpu_sah.cpp): an 8-wide BVH over the same
-// primitive boxes built with the surface-area heuristic, in the same
-// format; leaves hold at most max_leaf primitives.  Boxes and centroids must
+// primitive boxes, a binary surface-area-heuristic tree collapsed by a
+// cost-optimal dynamic program, in the same format; leaves hold at most
+// max_leaf primitives.  Boxes and centroids must
 // be finite.
 void build_sah_bvh(uint32_t n, const PrimBox* boxes, const float* centroids, RefBvh& out,
                    size_t max_leaf = 2);
